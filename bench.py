@@ -1,0 +1,463 @@
+#!/usr/bin/env python
+"""Benchmark of the graph-search hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload cfg3|cfg2|cfg1] [--L auto|<int>] [--nq Q] [--scale S]
+
+Workload (default): the 1.2M x 200 angular configuration -- seeded
+50-component Gaussian mixture, unit-normalised, inner product, K = 100, an
+NSG-style graph with out-degree <= 32 built on the device, 10k queries per
+GPU.  The beam width L is the smallest of the configuration's values (200,
+400, then 800) whose recall@10 against exact brute force is >= 0.95.
+
+One step = one batched persistent search over the whole query batch, with
+base, graph and queries resident in HBM (`value`, timed with CUDA events on
+the launching stream; the 960 MB base is larger than L2).  `e2e` times the
+public C ABI call with pinned host buffers (query upload and result download
+inside the timed region).  The plain per-query GPU path (one launch per
+query) is timed on a sample beside it.  `cpu_baseline` is the reference's
+own SearchArraySimulation (compiled from its sources, -Ofast) on the host
+cores over a bounded sample.
+
+--impl reference times that reference CPU search alone as the reference arm
+(same workload; rank 0 only under torchrun).
+
+Multi-GPU (torchrun, one rank per GPU): every rank holds a replica of the
+index and searches its own 10k queries (weak scaling, no device collective);
+time is the maximum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "QPS at recall@10≥0.95, batched vs plain GPU search; p50/p99 online latency"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def log(*a):
+    print("[bench]", *a, file=sys.stderr, flush=True)
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawTextHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="cfg3", choices=["cfg1", "cfg2", "cfg3"])
+    ap.add_argument("--L", default="auto")
+    ap.add_argument("--nq", type=int, default=10000, help="queries per GPU")
+    ap.add_argument("--scale", type=float, default=1.0, help="base size fraction (profiling)")
+    ap.add_argument("--plain-sample", type=int, default=300)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args(argv)
+
+
+# --------------------------------------------------------------- plumbing
+class Dist:
+    def __init__(self, backend):
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = False
+        if self.world > 1:
+            import torch.distributed as dist
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+            self.pg = True
+
+    def barrier(self):
+        if self.pg:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max(self, v, device=None):
+        from scattersearch_b200.replicas import max_over_ranks
+        return max_over_ranks(v, device) if self.pg else float(v)
+
+    def close(self):
+        if self.pg:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) while the timed region runs."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i]
+                          and "Not" not in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def measured_hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# --------------------------------------------------------------- workload
+def workload_spec(name):
+    if name == "cfg3":
+        return dict(cfg=3, Ls=[200, 400, 800], K=100, desc="1.2Mx200 angular (IP), K=100")
+    if name == "cfg2":
+        return dict(cfg=2, Ls=[64, 128, 256], K=10, desc="1Mx128 uint8-valued, L2, K=10")
+    return dict(cfg=1, Ls=[100, 200], K=10, desc="100kx200 L2, K=10")
+
+
+def build_workload(args, rank, world, device):
+    """Seeded data, NSG-style graph and exact ground truth (setup, untimed)."""
+    import torch
+    from scattersearch_b200 import datasets, graph
+    spec = workload_spec(args.workload)
+    t0 = time.time()
+    w = datasets.config(spec["cfg"], scale=args.scale, n_queries=args.nq * world)
+    queries = np.ascontiguousarray(w.queries[rank * args.nq:(rank + 1) * args.nq])
+    log(f"data {w.base.shape} queries {queries.shape} in {time.time() - t0:.1f}s")
+    t0 = time.time()
+    X = torch.from_numpy(w.base).to(device)
+    adj, ep = graph.build_graph(X, R=w.graph_R, knn_k=w.graph_knn, device=device)
+    log(f"graph R={w.graph_R} ep={ep} mean degree {(adj != 0xFFFFFFFF).sum(1).mean():.1f} "
+        f"in {time.time() - t0:.1f}s")
+    t0 = time.time()
+    Q = torch.from_numpy(queries).to(device)
+    gt, _ = graph.bruteforce(X, Q, 10, w.metric)
+    log(f"ground truth in {time.time() - t0:.1f}s")
+    return dict(spec=spec, w=w, X=X, queries=queries, Q=Q, adj=adj, ep=ep,
+                gt=gt.cpu().numpy(), metric=w.metric, K=spec["K"])
+
+
+def recall_at_10(ids, gt):
+    ids = np.asarray(ids)[:, :10].astype(np.int64)
+    hit = [(np.isin(ids[i], gt[i])).sum() for i in range(len(ids))]
+    return float(np.mean(hit) / 10.0)
+
+
+# -------------------------------------------------------- reference arm
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def time_reference(wl, L, seconds, fast=True, warm=1):
+    """Reference SearchArraySimulation on the host cores over a bounded
+    sample; returns (qps, sample size, ids of the sample, threads)."""
+    from oracle import oracle as O
+    th = cpu_threads()
+    ref = O.RefIndex(wl["w"].base, wl["metric"], wl["adj"], wl["ep"], fast=fast)
+    K = wl["K"]
+    q = wl["queries"]
+    probe = min(len(q), max(8 * th, 32))
+    t0 = time.perf_counter()
+    ref.search(q[:probe], K, L, nthreads=th)
+    rate = probe / max(1e-6, time.perf_counter() - t0)
+    sample = int(min(len(q), max(probe, rate * seconds)))
+    for _ in range(warm):
+        ref.search(q[:min(sample, probe)], K, L, nthreads=th)
+    t0 = time.perf_counter()
+    ids = ref.search(q[:sample], K, L, nthreads=th)
+    dt = time.perf_counter() - t0
+    ref.close()
+    return sample / dt, sample, ids, th
+
+
+def run_reference_arm(args):
+    d = Dist("gloo")
+    if d.rank != 0:
+        d.close()
+        return 0
+    import torch
+    from oracle import oracle as O
+    if not O.have_reference(fast=True):
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/libssref_fast.so was not built"}))
+        return 0
+    device = torch.device("cuda", d.local_rank) if torch.cuda.is_available() else "cpu"
+    wl = build_workload(args, 0, 1, device)
+    L = choose_L_reference(args, wl)
+    th = cpu_threads()
+    ref = O.RefIndex(wl["w"].base, wl["metric"], wl["adj"], wl["ep"], fast=True)
+    K, q = wl["K"], wl["queries"]
+    probe = min(len(q), max(8 * th, 32))
+    t0 = time.perf_counter()
+    ref.search(q[:probe], K, L, nthreads=th)
+    rate = probe / max(1e-6, time.perf_counter() - t0)
+    per_step = int(min(len(q), max(probe, rate * args.cpu_seconds / 2)))
+    for _ in range(args.warmup):
+        ref.search(q[:per_step], K, L, nthreads=th)
+    times = []
+    ids = None
+    for s in range(args.steps):
+        t0 = time.perf_counter()
+        ids = ref.search(q[:per_step], K, L, nthreads=th)
+        times.append(time.perf_counter() - t0)
+    ref.close()
+    total = sum(times)
+    qps = per_step * args.steps / total
+    rec = recall_at_10(ids, wl["gt"][:per_step])
+    sample = f"first {per_step} of {len(q)} queries per step, K={K}, L={L}"
+    out = {
+        "impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": wl["w"].name + " (synthetic, seeded)",
+        "config": {"workload": wl["spec"]["desc"], "K": K, "L": L, "nq_per_step": per_step,
+                   "recall@10": rec, "graph": "NSG-style, R<=32, built on the device (setup)"},
+        "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": th, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+    return 0
+
+
+def choose_L_reference(args, wl):
+    if args.L != "auto":
+        return int(args.L)
+    # same rule as our arm: smallest configured L whose GPU-free recall check
+    # passes is not affordable on the host, so use the GPU search to pick it
+    # when the library is present, else the largest configured L.
+    try:
+        from scattersearch_b200 import ANNSearch
+        idx = ANNSearch(wl["X"].shape[1], wl["X"].shape[0], wl["X"], wl["metric"],
+                        base_on_device=True)
+        idx.SetGraph(wl["adj"], wl["ep"])
+        L = pick_L(idx, wl)[0]
+        idx.close()
+        return L
+    except Exception as e:  # library missing: fall back to the configured maximum
+        log(f"L selection without the GPU library ({e}); using the largest configured L")
+        return wl["spec"]["Ls"][-1]
+
+
+# -------------------------------------------------------------- our arm
+def pick_L(idx, wl, target=0.95):
+    res = []
+    for L in wl["spec"]["Ls"]:
+        ids, _ = idx.search_batch(wl["queries"], wl["K"], L)
+        r = recall_at_10(ids, wl["gt"])
+        res.append((L, r))
+        log(f"L={L} recall@10={r:.4f}")
+        if r >= target:
+            return L, r, res
+    return res[-1][0], res[-1][1], res
+
+
+def run_ours(args):
+    import torch
+    d = Dist("nccl")
+    torch.cuda.set_device(d.local_rank)
+    device = torch.device("cuda", d.local_rank)
+    from scattersearch_b200 import ANNSearch
+    wl = build_workload(args, d.rank, d.world, device)
+    K = wl["K"]
+    nq, dim = wl["queries"].shape
+    idx = ANNSearch(dim, wl["X"].shape[0], wl["X"], wl["metric"], base_on_device=True)
+    idx.SetGraph(wl["adj"], wl["ep"])
+
+    if args.L == "auto":
+        L, rec, sweep = pick_L(idx, wl)
+    else:
+        L = int(args.L)
+        ids, _ = idx.search_batch(wl["queries"], K, L)
+        rec, sweep = recall_at_10(ids, wl["gt"]), []
+    # every rank must use the same L
+    if d.pg:
+        import torch.distributed as dist
+        t = torch.tensor([L], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        L = int(t.item())
+
+    Qd = wl["Q"]
+    ids_d = torch.empty((nq, K), dtype=torch.int32, device=device)
+    dist_d = torch.empty((nq, K), dtype=torch.float32, device=device)
+    ndc_d = torch.empty(nq, dtype=torch.int32, device=device)
+    hops_d = torch.empty(nq, dtype=torch.int32, device=device)
+    stream = torch.cuda.current_stream()
+
+    def step(with_stats=False):
+        idx.search_batch_device(Qd, nq, ids_d, dist_d, K=K, L=L,
+                                ndc=ndc_d if with_stats else None,
+                                hops=hops_d if with_stats else None, stream=stream.cuda_stream)
+
+    # stats pass (same traversal; gives the algorithmic bytes)
+    step(with_stats=True)
+    torch.cuda.synchronize()
+    if idx.batch_status():
+        raise RuntimeError("device batch reported failed queries")
+    ndc = ndc_d.cpu().numpy().astype(np.int64)
+    hops = hops_d.cpu().numpy().astype(np.int64)
+    rstride = idx.rstride
+    bytes_per_step = float(ndc.sum() * 4 * dim + hops.sum() * 4 * rstride + nq * 4 * dim)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    d.barrier()
+    sampler = ClockSampler(d.local_rank)
+    sampler.start()
+    torch.cuda.nvtx.range_push("timed")
+    evs = []
+    for _ in range(args.steps):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        step()
+        e.record(stream)
+        evs.append((s, e))
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    d.barrier()
+    clocks = sampler.stop()
+    step_ms = [s.elapsed_time(e) for s, e in evs]
+    total_s = d.max(sum(step_ms) / 1000.0, device)
+    qps = nq * d.world * args.steps / total_s
+    ids_np = ids_d.cpu().numpy().view(np.uint32)
+    rec_timed = recall_at_10(ids_np, wl["gt"])
+
+    # e2e: public C ABI with pinned host buffers
+    qh = torch.empty((nq, dim), dtype=torch.float32).pin_memory()
+    qh.numpy()[:] = wl["queries"]
+    ih = torch.empty((nq, K), dtype=torch.int32).pin_memory()
+    dh = torch.empty((nq, K), dtype=torch.float32).pin_memory()
+    qn, idn, dn = qh.numpy(), ih.numpy().view(np.uint32), dh.numpy()
+    for _ in range(max(1, args.warmup)):
+        idx.search_batch(qn, K, L, out_ids=idn, out_dists=dn)
+    d.barrier()
+    torch.cuda.synchronize()
+    e2e_t = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        idx.search_batch(qn, K, L, out_ids=idn, out_dists=dn)
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_s = d.max(sum(e2e_t), device)
+    e2e_qps = nq * d.world * args.steps / e2e_s
+    same_ids = bool(np.array_equal(idn, ids_np))
+
+    # plain per-query GPU path on a sample
+    ns = min(args.plain_sample, nq)
+    for i in range(min(8, ns)):
+        idx.search(wl["queries"][i], K, L)
+    t0 = time.perf_counter()
+    plain_ids = np.empty((ns, K), dtype=np.uint32)
+    for i in range(ns):
+        plain_ids[i], _ = idx.search(wl["queries"][i], K, L)
+    plain_s = time.perf_counter() - t0
+    plain_qps = ns / plain_s
+    plain_same = bool(np.array_equal(plain_ids, ids_np[:ns]))
+
+    peak, peak_kind = measured_hbm_peak()
+    mean_step_s = sum(step_ms) / len(step_ms) / 1000.0
+    achieved = bytes_per_step / mean_step_s / 1e9
+
+    out = {
+        "metric": METRIC, "value": qps, "unit": "queries/s", "n_gpus": d.world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total_s / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": wl["w"].name + " (synthetic, seeded numpy; graph built on the device)",
+        "config": {"workload": wl["spec"]["desc"] + f", {nq} queries per GPU, batched persistent",
+                   "K": K, "L": L, "recall@10": rec_timed, "L_sweep": sweep,
+                   "base": list(wl["X"].shape), "graph_R": int(wl["w"].graph_R),
+                   "mean_degree": float((wl["adj"] != 0xFFFFFFFF).sum(1).mean()),
+                   "l2": "inputs larger than L2 (base %.0f MB > 126 MB L2)"
+                         % (wl["X"].numel() * 4 / 1e6),
+                   "parallelism": f"replicas x{d.world}, queries sharded"},
+        "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": nq * dim * 4,
+                "d2h_bytes_per_step": nq * K * 8, "ids_equal_device_path": same_ids},
+        "plain_gpu": {"value": plain_qps, "unit": "queries/s", "sample": ns,
+                      "ids_equal_batched": plain_same,
+                      "batched_over_plain": qps / d.world / plain_qps},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_query": bytes_per_step / nq,
+                     "ndc_per_query": float(ndc.mean()), "hops_per_query": float(hops.mean()),
+                     "distance_evals_per_s": float(ndc.sum()) / mean_step_s},
+        "gpu_launches": args.steps,
+        "clocks": clocks,
+    }
+    if d.rank == 0 and d.world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        kind = "reference" if O.have_reference(fast=True) else None
+        if kind:
+            cqps, sample, cids, th = time_reference(wl, L, args.cpu_seconds)
+            out["cpu_baseline"] = {
+                "value": cqps, "unit": "queries/s", "cores": th, "kind": kind,
+                "sample": f"first {sample} of {nq} queries, K={K}, L={L}, reference "
+                          "SearchArraySimulation built -Ofast, OpenMP over queries",
+                "ids_equal_gpu_fraction": float((cids == ids_np[:sample]).all(1).mean())}
+        else:
+            out["cpu_baseline"] = None
+    idx.close()
+    if d.rank == 0:
+        print(json.dumps(out))
+    d.close()
+    return 0
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

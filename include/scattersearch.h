@@ -1,0 +1,203 @@
+/*
+ * scattersearch.h -- C ABI of the B200 graph search library
+ * (libscattersearch_b200.so).
+ *
+ * The reference (ScatterSearch) is a C++ class, ANNSearch
+ * (include/annsearch.h:37-84), used in-process by its benchmark drivers.  Each
+ * entry point below replaces one member of that class or one loop of its
+ * drivers; the comment on each names the reference code it replaces.
+ * include/scattersearch/annsearch.hpp wraps these calls in a header-only C++
+ * class with the reference's member names, so reference-style drivers compile
+ * against it unchanged.
+ *
+ * Conventions
+ *   - Every call returns an ss_status (0 = SS_OK).  On failure the message is
+ *     available from ss_last_error(handle) (or ss_last_error(NULL) for calls
+ *     that failed before a handle existed).  No C++ exception crosses the ABI.
+ *   - Host pointers are plain caller-owned buffers.  Calls with a _device
+ *     suffix take device pointers and a cudaStream_t passed as void*.
+ *   - A handle may be shared by several host threads: concurrent ss_search /
+ *     ss_search_batch calls on one handle are safe (each call borrows its own
+ *     stream and staging buffers).  Graph loading must not overlap searches.
+ *   - Metric values follow the reference's enum Metric {L2, INNER_PRODUCT}
+ *     (include/annsearch.h:22-26).  Inner-product distances are returned
+ *     negated, as distance_ip_avx does (src/distance.cpp:148).
+ *   - Result slots the search never filled (only possible on tiny or
+ *     disconnected graphs) hold id 0 and distance 0, the value-initialised
+ *     Neighbor of src/annsearch.cpp:193.
+ */
+#ifndef SCATTERSEARCH_H
+#define SCATTERSEARCH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ss_index ss_index;
+
+enum ss_metric { SS_METRIC_L2 = 0, SS_METRIC_INNER_PRODUCT = 1 };
+
+enum ss_status {
+  SS_OK = 0,
+  SS_ERR_INVALID_ARGUMENT = 1, /* bad size, K > L, null pointer, ...           */
+  SS_ERR_IO = 2,               /* file could not be opened or read            */
+  SS_ERR_FORMAT = 3,           /* malformed .nsg / .fbin / ground-truth file  */
+  SS_ERR_NO_GRAPH = 4,         /* search before a graph was loaded            */
+  SS_ERR_CUDA = 5,             /* CUDA runtime error (message has details)    */
+  SS_ERR_OUT_OF_MEMORY = 6,    /* device or host allocation failed            */
+  SS_ERR_UNSUPPORTED = 7,      /* parameter outside the compiled limits       */
+  SS_ERR_SEARCH_LIMIT = 8      /* a query hit the device hop limit            */
+};
+
+/* Largest beam width (pool size L) and graph degree the kernels accept. */
+#define SS_MAX_L 4096
+#define SS_MAX_DEGREE 128
+/* Largest number of expansions per step of ss_search_intra. */
+#define SS_MAX_INTRA_WIDTH 16
+
+/* ---- index lifetime ---------------------------------------------------- */
+
+/* Replaces ANNSearch::ANNSearch(unsigned dim, unsigned num, float *base,
+ * Metric m) (include/annsearch.h:40, src/annsearch.cpp:11-58).  Unlike the
+ * reference, which borrows `base`, the rows are copied into device memory
+ * (zero-padded to a multiple of 8 floats); the caller may free `base_host`
+ * after the call.  device: CUDA ordinal, or -1 for the current device. */
+int ss_create(uint32_t dim, uint32_t num, const float *base_host, int metric, int device,
+              ss_index **out);
+
+/* Same, with `base_dev` already on the device (num x dim floats, row-major,
+ * 16-byte aligned).  The rows are copied; the caller keeps ownership. */
+int ss_create_from_device(uint32_t dim, uint32_t num, const float *base_dev, int metric,
+                          int device, ss_index **out);
+
+/* Replaces ANNSearch::~ANNSearch (src/annsearch.cpp:60-62).  Frees every
+ * device allocation of the handle.  NULL is ignored. */
+void ss_destroy(ss_index *h);
+
+/* ---- graph ----------------------------------------------------------- */
+
+/* Replaces ANNSearch::LoadGraph (src/annsearch.cpp:64-80).  Reads the NSG
+ * file format: u32 width (ignored), u32 entry point, then per node u32 k and
+ * k u32 neighbour ids, until end of file.  Unlike the reference, a missing
+ * file, a truncated record, a node count different from `num`, or an id
+ * >= num is reported (SS_ERR_IO / SS_ERR_FORMAT) instead of ignored. */
+int ss_load_graph(ss_index *h, const char *path);
+
+/* Sets the graph from memory; replaces assigning the public members
+ * `graph` and `default_ep` (include/annsearch.h:77, :82).  adj is n x
+ * rstride uint32 on the host; each row is a prefix of neighbour ids followed
+ * by 0xFFFFFFFF padding.  n must equal the index's num. */
+int ss_set_graph(ss_index *h, const uint32_t *adj, uint32_t n, uint32_t rstride,
+                 uint32_t entry_point);
+
+/* Reads back the graph shape: node count, largest degree, entry point
+ * (default_ep, include/annsearch.h:77) and the padded row stride used on the
+ * device.  Any output pointer may be NULL. */
+int ss_graph_info(const ss_index *h, uint32_t *n, uint32_t *max_degree, uint32_t *entry_point,
+                  uint32_t *rstride);
+
+/* Copies the device adjacency back to the host (n x rstride uint32). */
+int ss_get_graph(ss_index *h, uint32_t *adj, uint32_t rstride);
+
+/* ---- search ------------------------------------------------------------ */
+
+/* Replaces ANNSearch::SearchArraySimulation(query, query_id, K, L, flags,
+ * indices) (src/annsearch.cpp:182-259): best-first search from the entry
+ * point with a pool of L, returning the K nearest in ascending distance.
+ * The visited set lives on the device, so the reference's caller-owned
+ * `flags` bitset has no counterpart.  One query per launch: this is the
+ * plain per-query GPU path.  ids: K uint32; dists: K floats (may be NULL).
+ * Requires 1 <= K <= L <= SS_MAX_L. */
+int ss_search(ss_index *h, const float *query, int K, int L, uint32_t *ids, float *dists);
+
+/* Replaces the drivers' query loop around SearchArraySimulation
+ * (tests/search.cpp:75-85; race-free per-thread visited sets as in
+ * tests/intraxinter.cpp:74-86).  All nq queries go to one persistent kernel
+ * that pulls queries from a device work queue; results are identical to nq
+ * calls of ss_search.  queries: nq x dim; ids/dists: nq x K. */
+int ss_search_batch(ss_index *h, const float *queries, uint32_t nq, int K, int L, uint32_t *ids,
+                    float *dists);
+
+/* Batched search with per-query K and L (Ks[i], Ls[i]); query i's results
+ * start at offset sum(Ks[0..i)) of ids/dists.  Results are identical to
+ * ss_search(query i, Ks[i], Ls[i]). */
+int ss_search_batch_uneven(ss_index *h, const float *queries, uint32_t nq, const int32_t *Ks,
+                           const int32_t *Ls, uint32_t *ids, float *dists);
+
+/* Device-resident batched search on `stream` (a cudaStream_t, NULL for the
+ * legacy default stream); asynchronous: returns after enqueueing.
+ * queries: nq x dim floats on the device.  Either (Ks, Ls, out_off) are
+ * device arrays of length nq, or they are NULL and K, L apply to all queries
+ * with query i's results at i*K.  ndc / hops (device, nq uint32, may be NULL)
+ * receive each query's distance evaluations and expansions.  Validation of
+ * per-query K/L happens on the device: a query with invalid K/L or one that
+ * hits the hop limit leaves its status nonzero, readable with
+ * ss_batch_status. */
+int ss_search_batch_device(ss_index *h, const float *queries, uint32_t nq, const int32_t *Ks,
+                           const int32_t *Ls, const int64_t *out_off, int K, int L, int L_max,
+                           uint32_t *ids, float *dists, uint32_t *ndc, uint32_t *hops,
+                           void *stream);
+
+/* After a synchronised ss_search_batch_device: number of queries of the last
+ * device batch on this handle whose status was nonzero. */
+int ss_batch_status(ss_index *h, uint32_t *failed_queries);
+
+/* Replaces ANNSearch::MultiThreadSearchArraySimulation[WithET]
+ * (src/annsearch.cpp:532-699, :839-1025): one query searched by a CTA of
+ * `num_threads` warps (1..SS_MAX_INTRA_WIDTH), each step expanding the
+ * num_threads best unexplored pool entries at once.  Acceptance, merge and
+ * termination rules are those of ss_search, so num_threads == 1 returns
+ * exactly the ss_search result; larger widths trade extra distance
+ * evaluations for fewer dependent steps, as the reference's intra-query
+ * threads do. */
+int ss_search_intra(ss_index *h, const float *query, int K, int L, int num_threads, uint32_t *ids,
+                    float *dists);
+
+/* Batch of queries, each searched by its own CTA of num_threads warps
+ * (config: small batches, several candidates expanded per step). */
+int ss_search_intra_batch(ss_index *h, const float *queries, uint32_t nq, int K, int L,
+                          int num_threads, uint32_t *ids, float *dists);
+
+/* Device-pointer form of ss_search_intra_batch (asynchronous on `stream`). */
+int ss_search_intra_batch_device(ss_index *h, const float *queries, uint32_t nq, int K, int L,
+                                 int num_threads, uint32_t *ids, float *dists, uint32_t *ndc,
+                                 uint32_t *hops, void *stream);
+
+/* Launch tuning of the batched warp-per-query kernel, normally chosen by the
+ * autotuner (scattersearch_b200.autotune) per (dim, degree, L); no
+ * counterpart in the reference, whose only knobs are #defines and argv.
+ * warps_per_block: query teams per CTA (1, 2, 4 or 8); hash_cap: visited-hash
+ * slots per query (0 = automatic, 16 x L rounded up to a power of two);
+ * blocks_per_sm_cap: limit on resident CTAs per SM (0 = occupancy limit). */
+int ss_set_tuning(ss_index *h, int warps_per_block, int hash_cap, int blocks_per_sm_cap);
+
+/* ---- host I/O (util.cpp) ---------------------------------------------- */
+
+/* Replaces load_fbin (src/util.cpp:40-70): u32 num, u32 dim, then num x dim
+ * f32.  *data is malloc'd with 8 floats of zeroed slack after the rows, as
+ * the reference allocates; free it with ss_free.  Short files are reported. */
+int ss_load_fbin(const char *path, float **data, uint32_t *num, uint32_t *dim);
+
+/* Replaces load_groundtruth (src/util.cpp:72-93): u32 nq, u32 K, then
+ * nq x K u32.  *ids is malloc'd; free with ss_free. */
+int ss_load_groundtruth(const char *path, uint32_t **ids, uint32_t *nq, uint32_t *k);
+
+void ss_free(void *p);
+
+/* ---- diagnostics ----------------------------------------------------- */
+
+/* Message of the last failed call on `h` (or on this thread when h is
+ * NULL).  The string stays valid until the next failing call. */
+const char *ss_last_error(const ss_index *h);
+
+/* Library version string, e.g. "scattersearch_b200 0.1 sm_100a". */
+const char *ss_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SCATTERSEARCH_H */

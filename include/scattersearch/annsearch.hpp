@@ -1,0 +1,151 @@
+// Header-only C++ drop-in for the reference's ANNSearch (include/annsearch.h:37-84)
+// over the C ABI of libscattersearch_b200.so (include/scattersearch.h).
+//
+// Member names, argument order and meaning follow the reference so its
+// drivers compile against this class; include/scattersearch/compat/ puts the
+// names in the global namespace for that purpose.  Differences:
+//   * the caller's `flags` bitset is accepted as any type with reset() and
+//     only reset (the reference resets it at src/annsearch.cpp:258); the
+//     visited set lives on the GPU;
+//   * failures print the library's message and exit(-1), the reference's
+//     error behaviour for loaders (src/util.cpp:42-47) applied to every call
+//     (its LoadGraph ignores a failed open, src/annsearch.cpp:66);
+//   * `graph` (vector<vector<unsigned>>) is not kept on the host;
+//     graph_table() copies the device adjacency out on demand.
+#ifndef SCATTERSEARCH_ANNSEARCH_HPP
+#define SCATTERSEARCH_ANNSEARCH_HPP
+
+#include <scattersearch.h>
+
+#include <atomic>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+
+namespace scattersearch {
+
+enum Metric { L2 = SS_METRIC_L2, INNER_PRODUCT = SS_METRIC_INNER_PRODUCT };
+
+inline void die_on_error(int rc, const ss_index *h, const char *what) {
+  if (rc != SS_OK) {
+    std::fprintf(stderr, "%s failed (%d): %s\n", what, rc, ss_last_error(h));
+    std::exit(-1);
+  }
+}
+
+// load_fbin (src/util.cpp:40-70): rows plus 8 floats of zeroed slack.
+inline void load_fbin(const char *filename, float *&data, unsigned &num, unsigned &dim) {
+  uint32_t n = 0, d = 0;
+  die_on_error(ss_load_fbin(filename, &data, &n, &d), nullptr, "load_fbin");
+  num = n;
+  dim = d;
+}
+
+// load_groundtruth (src/util.cpp:72-93).
+inline void load_groundtruth(const char *filename, std::vector<std::vector<unsigned>> &gt) {
+  uint32_t *ids = nullptr, nq = 0, k = 0;
+  die_on_error(ss_load_groundtruth(filename, &ids, &nq, &k), nullptr, "load_groundtruth");
+  for (uint32_t i = 0; i < nq; ++i) gt.emplace_back(ids + (size_t)i * k, ids + (size_t)(i + 1) * k);
+  ss_free(ids);
+}
+
+class ANNSearch {
+ public:
+  // ANNSearch(dim, num, base, metric), src/annsearch.cpp:11-58.  The rows
+  // are copied to the GPU; `base` stays the caller's.
+  ANNSearch(unsigned dim, unsigned num, float *base, Metric m, int device = -1)
+      : dimension(dim), base_num(num), base_data(base) {
+    die_on_error(ss_create(dim, num, base, (int)m, device, &handle), nullptr, "ANNSearch");
+  }
+  ~ANNSearch() { ss_destroy(handle); }
+  ANNSearch(const ANNSearch &) = delete;
+  ANNSearch &operator=(const ANNSearch &) = delete;
+
+  // src/annsearch.cpp:64-80
+  void LoadGraph(const char *filename) {
+    die_on_error(ss_load_graph(handle, filename), handle, "LoadGraph");
+    uint32_t ep = 0;
+    ss_graph_info(handle, nullptr, nullptr, &ep, nullptr);
+    default_ep = ep;
+  }
+  // src/annsearch.cpp:82-101
+  void LoadGroundtruth(const char *filename) { load_groundtruth(filename, groundtruth); }
+
+  // Graph from an n x rstride table padded with 0xFFFFFFFF.
+  void SetGraph(const std::vector<uint32_t> &adj, unsigned rstride, unsigned ep) {
+    die_on_error(ss_set_graph(handle, adj.data(), (uint32_t)base_num, rstride, ep), handle,
+                 "SetGraph");
+    default_ep = ep;
+  }
+
+  // src/annsearch.cpp:182-259.  `indices` must hold at least K entries.
+  template <class Flags>
+  void SearchArraySimulation(const float *query, unsigned /*query_id*/, int K, int L, Flags &flags,
+                             std::vector<unsigned> &indices) {
+    if ((int)indices.size() < K) indices.resize(K);
+    die_on_error(ss_search(handle, query, K, L, reinterpret_cast<uint32_t *>(indices.data()),
+                           nullptr),
+                 handle, "SearchArraySimulation");
+    flags.reset();
+  }
+
+  // src/annsearch.cpp:532-699: num_threads warps expand num_threads
+  // candidates per step.
+  template <class Flags>
+  void MultiThreadSearchArraySimulation(const float *query, unsigned /*query_id*/, int K, int L,
+                                        int num_threads, Flags &flags,
+                                        std::vector<unsigned> &indices) {
+    if ((int)indices.size() < K) indices.resize(K);
+    die_on_error(ss_search_intra(handle, query, K, L, num_threads,
+                                 reinterpret_cast<uint32_t *>(indices.data()), nullptr),
+                 handle, "MultiThreadSearchArraySimulation");
+    flags.reset();
+  }
+
+  // src/annsearch.cpp:839-1025.  All warps of the CTA step in lock step, so
+  // there is no idle thread for the election / early termination to stop.
+  template <class Flags>
+  void MultiThreadSearchArraySimulationWithET(const float *query, unsigned query_id, int K, int L,
+                                              int num_threads, Flags &flags,
+                                              std::vector<unsigned> &indices) {
+    MultiThreadSearchArraySimulation(query, query_id, K, L, num_threads, flags, indices);
+  }
+
+  // Batched extension: nq queries, one persistent launch.  ids: nq*K.
+  void SearchBatch(const float *queries, unsigned nq, int K, int L, std::vector<unsigned> &ids,
+                   std::vector<float> *dists = nullptr) {
+    ids.resize((size_t)nq * K);
+    if (dists) dists->resize((size_t)nq * K);
+    die_on_error(ss_search_batch(handle, queries, nq, K, L,
+                                 reinterpret_cast<uint32_t *>(ids.data()),
+                                 dists ? dists->data() : nullptr),
+                 handle, "SearchBatch");
+  }
+
+  std::vector<uint32_t> graph_table(unsigned rstride) const {
+    std::vector<uint32_t> out((size_t)base_num * rstride);
+    die_on_error(ss_get_graph(handle, out.data(), rstride), handle, "graph_table");
+    return out;
+  }
+
+ public:
+  // Public members of the reference (include/annsearch.h:58-83).  The
+  // counters exist so drivers that print them compile; the GPU path does not
+  // update them.
+  std::atomic<int> hop_count{0};
+  float ub_ratio = 0;
+  int64_t dist_comps = 0;
+  int64_t max_dist_comps = 0;
+  double time_expand_ = 0, time_merge_ = 0, time_seq_ = 0, time_total_ = 0;
+  unsigned default_ep = 0;
+  size_t dimension;
+  size_t base_num;
+  float *base_data;
+  std::vector<std::vector<unsigned>> groundtruth;
+  ss_index *handle = nullptr;
+};
+
+}  // namespace scattersearch
+
+#endif

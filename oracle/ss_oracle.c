@@ -1,0 +1,248 @@
+/*
+ * ss_oracle.c -- CPU restatement of ScatterSearch's graph search path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and
+ * bench.py's cpu_baseline leg may load this library, and only as the checker.
+ * The product (scattersearch_b200/) never links or calls it.
+ *
+ * Parity is pinned: tests/test_oracle.py checks every function here against
+ * the reference itself, compiled in place from its sources into oracle/_ref/
+ * (oracle/Makefile), and against the golden fixtures under tests/golden/ that
+ * tests/golden/make_golden.py produced from that compiled reference.
+ *
+ * Reference semantics restated (reference paths):
+ *   distance_l2sqr_avx   src/distance.cpp:19-56
+ *   distance_ip_avx      src/distance.cpp:115-149
+ *   InsertIntoPool       include/util.h:41-78   (upper-bound insert: ties keep
+ *                        the older entry first)
+ *   SearchArraySimulation src/annsearch.cpp:182-259
+ *
+ * The search is written in "batch-merge" form rather than the reference's
+ * insert-one-at-a-time loop.  The two are equivalent:
+ *   - the reference always expands the first unexplored slot below
+ *     min(L, size) (its k / nk bookkeeping, annsearch.cpp:218-253);
+ *   - a candidate is accepted iff d < pool[size-1] taken at the START of the
+ *     hop: the live threshold only shrinks inside a hop, and any candidate it
+ *     rejects would also fall past slot L in the merge below (annsearch.cpp:238);
+ *   - the new pool is the stable merge of the old pool and the accepted
+ *     candidates (old entries first on equal distance, candidates in adjacency
+ *     order), truncated to min(L, size + accepted) (util.h:56-75,
+ *     annsearch.cpp:242-243).
+ * One place the reference leaves the order open: std::sort of the initial
+ * pool (annsearch.cpp:215) is not stable.  Exactly tied initial distances are
+ * ordered here by adjacency position.
+ *
+ * Adjacency layout shared with the GPU path: n x rstride uint32, each row a
+ * prefix of neighbour ids followed by 0xFFFFFFFF padding.
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define SSO_NONE 0xFFFFFFFFu
+#define SSO_L2 0
+#define SSO_IP 1
+
+/* 8-lane distance model of distance.cpp:19-56 / :115-149.  D = dim rounded up
+ * to 8; when D % 16 == 8 the last 8-block is accumulated first (:42-45), then
+ * the 8-blocks in order (:47-51), each lane a separate mul and add with no
+ * fusion, then lanes summed left to right (:53).  Lanes past `dim` read 0. */
+float sso_distance(const float *a, const float *b, unsigned dim, int metric) {
+  unsigned nb = (dim + 7u) / 8u;
+  float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (unsigned t = 0; t < nb; ++t) {
+    unsigned blk = (nb & 1u) ? (t == 0 ? nb - 1 : t - 1) : t;
+    for (unsigned j = 0; j < 8; ++j) {
+      unsigned i = blk * 8 + j;
+      float x = i < dim ? a[i] : 0.0f;
+      float y = i < dim ? b[i] : 0.0f;
+      float p;
+      if (metric == SSO_L2) {
+        float df = x - y;
+        p = df * df;
+      } else {
+        p = x * y;
+      }
+      acc[j] = acc[j] + p;
+    }
+  }
+  float r = acc[0];
+  for (unsigned j = 1; j < 8; ++j) r = r + acc[j];
+  return metric == SSO_L2 ? r : -r;
+}
+
+typedef struct {
+  float d;
+  uint32_t id;
+  uint32_t explored;
+} sso_ent;
+
+/* Stable insertion sort by distance (ties keep input order). */
+static void sort_stable(sso_ent *e, unsigned n) {
+  for (unsigned i = 1; i < n; ++i) {
+    sso_ent v = e[i];
+    unsigned j = i;
+    while (j > 0 && e[j - 1].d > v.d) {
+      e[j] = e[j - 1];
+      --j;
+    }
+    e[j] = v;
+  }
+}
+
+/* Stable merge of pool[0,s) and cand[0,nc) into out, old first on ties,
+ * keeping at most cap entries.  Returns the merged length. */
+static unsigned merge_pool(const sso_ent *pool, unsigned s, const sso_ent *cand, unsigned nc,
+                           sso_ent *out, unsigned cap) {
+  unsigned i = 0, j = 0, o = 0;
+  while (o < cap && (i < s || j < nc)) {
+    if (j >= nc || (i < s && pool[i].d <= cand[j].d)) out[o++] = pool[i++];
+    else out[o++] = cand[j++];
+  }
+  return o;
+}
+
+typedef struct {
+  const float *base;
+  uint32_t n, dim;
+  const uint32_t *adj;
+  uint32_t rstride, ep;
+  int metric;
+} sso_index;
+
+/* Best-first search for one query, expanding up to W best unexplored entries
+ * per step.  W == 1 is exactly SearchArraySimulation (annsearch.cpp:182-259).
+ * For W > 1 (the several-candidates-per-step form, structured like
+ * ModifiedDeltaStepping annsearch.cpp:1632-1691) the acceptance threshold,
+ * stable merge and truncation rules are the W == 1 ones, and candidates are
+ * ordered by (expansion slot w, adjacency position m); the first occurrence of
+ * an id in that order is the one evaluated.
+ * visited: n bytes, all zero on entry, left dirty.  Returns 0. */
+static int search_one(const sso_index *ix, const float *q, int K, int L, int W, uint32_t *ids,
+                      float *dists, uint8_t *visited, uint32_t *ndc_out, uint32_t *hops_out,
+                      sso_ent *pool, sso_ent *tmp, sso_ent *cand) {
+  uint32_t ndc = 0, hops = 0;
+  const uint32_t *row = ix->adj + (size_t)ix->ep * ix->rstride;
+  unsigned s = 0;
+  /* initial pool: first min(L, deg(ep)) neighbours of ep, all marked visited
+   * (annsearch.cpp:188-192), distances, sort (:207-215) */
+  for (unsigned m = 0; m < ix->rstride && row[m] != SSO_NONE && s < (unsigned)L; ++m) {
+    uint32_t id = row[m];
+    visited[id] = 1;
+    pool[s].id = id;
+    pool[s].d = sso_distance(ix->base + (size_t)id * ix->dim, q, ix->dim, ix->metric);
+    pool[s].explored = 0;
+    ++s;
+    ++ndc;
+  }
+  sort_stable(pool, s);
+  for (;;) {
+    unsigned picks[64];
+    unsigned np = 0;
+    for (unsigned k = 0; k < s && np < (unsigned)W; ++k)
+      if (!pool[k].explored) picks[np++] = k;
+    if (np == 0) break;
+    float thr = pool[s - 1].d;
+    unsigned nc = 0;
+    for (unsigned w = 0; w < np; ++w) {
+      pool[picks[w]].explored = 1;
+      ++hops;
+      const uint32_t *nr = ix->adj + (size_t)pool[picks[w]].id * ix->rstride;
+      for (unsigned m = 0; m < ix->rstride && nr[m] != SSO_NONE; ++m) {
+        uint32_t id = nr[m];
+        if (visited[id]) continue;
+        visited[id] = 1;
+        float d = sso_distance(q, ix->base + (size_t)id * ix->dim, ix->dim, ix->metric);
+        ++ndc;
+        if (d >= thr) continue;
+        cand[nc].d = d;
+        cand[nc].id = id;
+        cand[nc].explored = 0;
+        ++nc;
+      }
+    }
+    sort_stable(cand, nc);
+    unsigned ns = merge_pool(pool, s, cand, nc, tmp, (unsigned)L);
+    memcpy(pool, tmp, ns * sizeof(sso_ent));
+    s = ns;
+  }
+  for (int i = 0; i < K; ++i) {
+    /* slots the pool never reached hold the value-initialised Neighbor
+     * (id 0, distance 0) of annsearch.cpp:193 */
+    ids[i] = (unsigned)i < s ? pool[i].id : 0u;
+    if (dists) dists[i] = (unsigned)i < s ? pool[i].d : 0.0f;
+  }
+  if (ndc_out) *ndc_out = ndc;
+  if (hops_out) *hops_out = hops;
+  return 0;
+}
+
+/* Searches nq queries (row-major nq x dim).  Per-query K and L (arrays of
+ * length nq, or NULL to use K0 / L0).  ids/dists are written at out_off[i]
+ * (or i*K0 when out_off is NULL).  W: expansions per step (1 = plain).
+ * nthreads > 1 parallelises across queries with OpenMP.  Returns 0, or -1 on
+ * bad arguments. */
+int sso_search_batch(const float *base, uint32_t n, uint32_t dim, int metric, const uint32_t *adj,
+                     uint32_t rstride, uint32_t ep, const float *queries, uint32_t nq,
+                     const int32_t *Ks, const int32_t *Ls, int K0, int L0, int W,
+                     const int64_t *out_off, uint32_t *ids, float *dists, uint32_t *ndc,
+                     uint32_t *hops, int nthreads) {
+  if (W < 1 || W > 64 || ep >= n) return -1;
+  sso_index ix = {base, n, dim, adj, rstride, ep, metric};
+  int Lmax = L0;
+  if (Ls)
+    for (uint32_t i = 0; i < nq; ++i) Lmax = Ls[i] > Lmax ? Ls[i] : Lmax;
+  int bad = 0;
+#pragma omp parallel num_threads(nthreads > 0 ? nthreads : 1) reduction(| : bad)
+  {
+    uint8_t *visited = (uint8_t *)calloc(n, 1);
+    sso_ent *pool = (sso_ent *)malloc(sizeof(sso_ent) * (size_t)(Lmax + 1));
+    sso_ent *tmp = (sso_ent *)malloc(sizeof(sso_ent) * (size_t)(Lmax + 1));
+    sso_ent *cand = (sso_ent *)malloc(sizeof(sso_ent) * (size_t)rstride * (size_t)W);
+#pragma omp for schedule(dynamic, 4)
+    for (long i = 0; i < (long)nq; ++i) {
+      int K = Ks ? Ks[i] : K0, L = Ls ? Ls[i] : L0;
+      int64_t off = out_off ? out_off[i] : (int64_t)i * K0;
+      if (K < 1 || K > L) {
+        bad = 1;
+        continue;
+      }
+      search_one(&ix, queries + (size_t)i * dim, K, L, W, ids + off, dists ? dists + off : NULL,
+                 visited, ndc ? ndc + i : NULL, hops ? hops + i : NULL, pool, tmp, cand);
+      memset(visited, 0, n);
+    }
+    free(visited);
+    free(pool);
+    free(tmp);
+    free(cand);
+  }
+  return bad ? -1 : 0;
+}
+
+/* Exact brute force top-k under the same distance model (ties by id). */
+int sso_bruteforce(const float *base, uint32_t n, uint32_t dim, int metric, const float *queries,
+                   uint32_t nq, int k, uint32_t *ids, float *dists, int nthreads) {
+#pragma omp parallel for num_threads(nthreads > 0 ? nthreads : 1) schedule(dynamic, 1)
+  for (long i = 0; i < (long)nq; ++i) {
+    sso_ent *best = (sso_ent *)malloc(sizeof(sso_ent) * (size_t)(k + 1));
+    int cnt = 0;
+    const float *q = queries + (size_t)i * dim;
+    for (uint32_t j = 0; j < n; ++j) {
+      float d = sso_distance(q, base + (size_t)j * dim, dim, metric);
+      if (cnt == k && d >= best[k - 1].d) continue;
+      int p = cnt < k ? cnt++ : k - 1;
+      while (p > 0 && best[p - 1].d > d) {
+        best[p] = best[p - 1];
+        --p;
+      }
+      best[p].d = d;
+      best[p].id = j;
+    }
+    for (int t = 0; t < k; ++t) {
+      ids[(size_t)i * k + t] = t < cnt ? best[t].id : SSO_NONE;
+      if (dists) dists[(size_t)i * k + t] = t < cnt ? best[t].d : 0.0f;
+    }
+    free(best);
+  }
+  return 0;
+}

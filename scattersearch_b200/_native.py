@@ -1,0 +1,90 @@
+"""ctypes binding of libscattersearch_b200.so (the C ABI in include/scattersearch.h).
+
+The binding fails loudly: importing a search entry point without the built
+library raises, and there is no CPU fallback anywhere in this package.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libscattersearch_b200.so")
+
+SS_OK = 0
+STATUS_NAMES = {
+    0: "SS_OK", 1: "SS_ERR_INVALID_ARGUMENT", 2: "SS_ERR_IO", 3: "SS_ERR_FORMAT",
+    4: "SS_ERR_NO_GRAPH", 5: "SS_ERR_CUDA", 6: "SS_ERR_OUT_OF_MEMORY", 7: "SS_ERR_UNSUPPORTED",
+    8: "SS_ERR_SEARCH_LIMIT",
+}
+SS_MAX_L = 4096
+SS_MAX_DEGREE = 128
+SS_MAX_INTRA_WIDTH = 16
+
+# Every function the header declares, with its ctypes signature.
+_vp = ctypes.c_void_p
+_u32 = ctypes.c_uint32
+_i32 = ctypes.c_int
+_f32p = ctypes.POINTER(ctypes.c_float)
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_hp = ctypes.POINTER(ctypes.c_void_p)
+
+SIGNATURES = {
+    "ss_create": (_i32, [_u32, _u32, _f32p, _i32, _i32, _hp]),
+    "ss_create_from_device": (_i32, [_u32, _u32, _vp, _i32, _i32, _hp]),
+    "ss_destroy": (None, [_vp]),
+    "ss_load_graph": (_i32, [_vp, ctypes.c_char_p]),
+    "ss_set_graph": (_i32, [_vp, _u32p, _u32, _u32, _u32]),
+    "ss_graph_info": (_i32, [_vp, _u32p, _u32p, _u32p, _u32p]),
+    "ss_get_graph": (_i32, [_vp, _u32p, _u32]),
+    "ss_search": (_i32, [_vp, _f32p, _i32, _i32, _u32p, _f32p]),
+    "ss_search_batch": (_i32, [_vp, _f32p, _u32, _i32, _i32, _u32p, _f32p]),
+    "ss_search_batch_uneven": (_i32, [_vp, _f32p, _u32, _i32p, _i32p, _u32p, _f32p]),
+    "ss_search_batch_device": (_i32, [_vp, _vp, _u32, _vp, _vp, _vp, _i32, _i32, _i32, _vp, _vp,
+                                      _vp, _vp, _vp]),
+    "ss_batch_status": (_i32, [_vp, _u32p]),
+    "ss_search_intra": (_i32, [_vp, _f32p, _i32, _i32, _i32, _u32p, _f32p]),
+    "ss_search_intra_batch": (_i32, [_vp, _f32p, _u32, _i32, _i32, _i32, _u32p, _f32p]),
+    "ss_search_intra_batch_device": (_i32, [_vp, _vp, _u32, _i32, _i32, _i32, _vp, _vp, _vp, _vp,
+                                            _vp]),
+    "ss_set_tuning": (_i32, [_vp, _i32, _i32, _i32]),
+    "ss_load_fbin": (_i32, [ctypes.c_char_p, ctypes.POINTER(_f32p), _u32p, _u32p]),
+    "ss_load_groundtruth": (_i32, [ctypes.c_char_p, ctypes.POINTER(_u32p), _u32p, _u32p]),
+    "ss_free": (None, [_vp]),
+    "ss_last_error": (ctypes.c_char_p, [_vp]),
+    "ss_version": (ctypes.c_char_p, []),
+}
+
+_lib = None
+
+
+class SearchError(RuntimeError):
+    """A C ABI call returned a nonzero ss_status."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m scattersearch_b200.build` "
+                "(there is no CPU fallback)")
+        l = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(l, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = l
+    return _lib
+
+
+def check(rc: int, handle=None) -> None:
+    if rc != SS_OK:
+        msg = lib().ss_last_error(handle)
+        raise SearchError(rc, msg.decode() if msg else "")

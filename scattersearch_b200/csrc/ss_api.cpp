@@ -1,0 +1,775 @@
+// Host side of the C ABI declared in include/scattersearch.h.
+//
+// Owns the device copies of the base rows and the adjacency, plans kernel
+// launches, and hands each concurrent caller its own stream and staging
+// buffers (the reference shares one ANNSearch between threads that each own
+// their visited bitset, tests/search.cpp:75-80; here the per-caller state is
+// a SearchCtx borrowed from a pool).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "scattersearch.h"
+#include "ss_internal.h"
+
+namespace {
+
+thread_local std::string tl_error;
+thread_local std::string tl_handle_error_copy;
+
+int fail(std::string *sink, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  tl_error = buf;
+  if (sink) *sink = buf;
+  return code;
+}
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  // Grows to at least `bytes`; new memory is zeroed when `zero` is set.
+  cudaError_t ensure(size_t bytes, bool zero = false) {
+    if (bytes <= cap) return cudaSuccess;
+    if (p) {
+      cudaFree(p);
+      p = nullptr;
+      cap = 0;
+    }
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return e;
+    }
+    cap = bytes;
+    if (zero) e = cudaMemset(p, 0, bytes);
+    return e;
+  }
+  template <class T>
+  T *as() const {
+    return static_cast<T *>(p);
+  }
+};
+
+// Per-caller launch state: one stream plus the buffers a search needs.
+struct SearchCtx {
+  cudaStream_t stream = nullptr;
+  DevBuf q, ids, dists, Ks, Ls, off, counter, status, ndc, hops, spill;
+  std::vector<int32_t> h_status;
+  ~SearchCtx() {
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+uint32_t round_up(uint32_t x, uint32_t m) { return (x + m - 1) / m * m; }
+
+}  // namespace
+
+struct ss_index {
+  int device = 0;
+  uint32_t dim = 0, n = 0, nb = 0;
+  int metric = 0;
+  int sm_count = 0;
+  DevBuf base;
+  DevBuf adj;
+  uint32_t rstride = 0, max_deg = 0, ep = 0;
+  bool has_graph = false;
+
+  std::mutex mu;  // guards err, contexts
+  std::string err;
+  std::vector<std::unique_ptr<SearchCtx>> ctx_all;
+  std::vector<SearchCtx *> ctx_free;
+
+  std::mutex dev_mu;  // device-batch scratch
+  SearchCtx dev_ctx;
+  uint32_t dev_last_nq = 0;
+
+  // launch tuning (set by the autotuner through ss_set_tuning)
+  int warps_per_block = 4;
+  int hash_cap_override = 0;
+  int blocks_per_sm_cap = 0;
+
+  ssb::GraphView view() const {
+    ssb::GraphView g;
+    g.base = base.as<const float>();
+    g.adj = adj.as<const uint32_t>();
+    g.n = n;
+    g.dim = dim;
+    g.nb = nb;
+    g.rstride = rstride;
+    g.ep = ep;
+    g.metric = metric;
+    return g;
+  }
+};
+
+namespace {
+
+int cuda_fail(ss_index *h, cudaError_t e, const char *what) {
+  return fail(h ? &h->err : nullptr, SS_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+int set_err(ss_index *h, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (h) {
+    std::lock_guard<std::mutex> lk(h->mu);
+    return fail(&h->err, code, "%s", buf);
+  }
+  return fail(nullptr, code, "%s", buf);
+}
+
+#define SS_CUDA(h, call, what)                         \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) {                           \
+      std::lock_guard<std::mutex> lk_((h)->mu);        \
+      return cuda_fail((h), e_, what);                 \
+    }                                                  \
+  } while (0)
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+SearchCtx *acquire_ctx(ss_index *h) {
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (!h->ctx_free.empty()) {
+    SearchCtx *c = h->ctx_free.back();
+    h->ctx_free.pop_back();
+    return c;
+  }
+  auto c = std::make_unique<SearchCtx>();
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+  SearchCtx *raw = c.get();
+  h->ctx_all.push_back(std::move(c));
+  return raw;
+}
+
+void release_ctx(ss_index *h, SearchCtx *c) {
+  std::lock_guard<std::mutex> lk(h->mu);
+  h->ctx_free.push_back(c);
+}
+
+struct CtxLease {
+  ss_index *h;
+  SearchCtx *c;
+  CtxLease(ss_index *hh) : h(hh), c(acquire_ctx(hh)) {}
+  ~CtxLease() {
+    if (c) release_ctx(h, c);
+  }
+};
+
+uint32_t spill_words(const ss_index *h) { return (h->n + 31) / 32; }
+
+int check_search_args(ss_index *h, int K, int L) {
+  if (!h) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null index handle");
+  if (!h->has_graph) return set_err(h, SS_ERR_NO_GRAPH, "no graph loaded");
+  if (K < 1 || L < 1 || K > L)
+    return set_err(h, SS_ERR_INVALID_ARGUMENT, "need 1 <= K <= L (got K=%d, L=%d)", K, L);
+  if (L > SS_MAX_L) return set_err(h, SS_ERR_UNSUPPORTED, "L=%d exceeds SS_MAX_L=%d", L, SS_MAX_L);
+  return SS_OK;
+}
+
+int status_to_error(ss_index *h, const int32_t *st, uint32_t nq) {
+  uint32_t bad = 0, hop = 0, full = 0, first = 0;
+  for (uint32_t i = 0; i < nq; ++i) {
+    if (st[i] != ssb::kStatusOk) {
+      if (bad == 0) first = i;
+      ++bad;
+      if (st[i] == ssb::kStatusHopLimit) ++hop;
+      if (st[i] == ssb::kStatusVisitedFull) ++full;
+    }
+  }
+  if (!bad) return SS_OK;
+  if (hop)
+    return set_err(h, SS_ERR_SEARCH_LIMIT, "%u queries hit the hop limit (first: %u)", hop, first);
+  if (full)
+    return set_err(h, SS_ERR_SEARCH_LIMIT, "%u queries overflowed the visited table (first: %u)",
+                   full, first);
+  return set_err(h, SS_ERR_INVALID_ARGUMENT, "%u queries had invalid K/L (first: %u)", bad, first);
+}
+
+// Persistent grid size for the warp kernel: every SM filled, never more
+// teams than queries.
+int persistent_blocks(ss_index *h, const ssb::SmemPlan &p, int wpb, uint32_t nq) {
+  int per_sm = ssb::warp_search_occupancy(h->view(), p, wpb);
+  if (per_sm <= 0) return 0;
+  if (h->blocks_per_sm_cap > 0) per_sm = std::min(per_sm, h->blocks_per_sm_cap);
+  long full = (long)per_sm * h->sm_count;
+  long need = ((long)nq + wpb - 1) / wpb;
+  return (int)std::max(1L, std::min(full, need));
+}
+
+int choose_wpb(ss_index *h, const ssb::SmemPlan &p) {
+  int wpb = h->warps_per_block;
+  // shared memory per CTA must fit the 227 KB opt-in limit
+  while (wpb > 1 && (size_t)p.words_per_team * 4 * wpb > 227 * 1024) wpb >>= 1;
+  return wpb;
+}
+
+// Core batched launch into caller-provided device buffers on `stream`.
+int launch_batch(ss_index *h, SearchCtx *c, const float *d_q, uint32_t nq, const int32_t *d_K,
+                 const int32_t *d_L, const int64_t *d_off, int K0, int L0, int L_max,
+                 uint32_t *d_ids, float *d_dists, uint32_t *d_ndc, uint32_t *d_hops,
+                 cudaStream_t stream, bool persistent) {
+  ssb::GraphView g = h->view();
+  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, h->hash_cap_override);
+  const int wpb = choose_wpb(h, plan);
+  if ((size_t)plan.words_per_team * 4 * wpb > 227 * 1024)
+    return set_err(h, SS_ERR_UNSUPPORTED, "L=%d needs %u bytes of shared memory per query",
+                   L_max, plan.words_per_team * 4);
+  int blocks = persistent ? persistent_blocks(h, plan, wpb, nq)
+                          : (int)((nq + (uint32_t)wpb - 1) / (uint32_t)wpb);
+  if (blocks <= 0) return set_err(h, SS_ERR_UNSUPPORTED, "search kernel cannot be resident");
+  const size_t slots = (size_t)blocks * wpb;
+  SS_CUDA(h, c->spill.ensure(slots * spill_words(h) * 4, true), "spill bitset allocation");
+  SS_CUDA(h, c->status.ensure((size_t)std::max(nq, 1u) * 4), "status allocation");
+  SS_CUDA(h, c->counter.ensure(16), "counter allocation");
+  ssb::BatchArgs a{};
+  a.queries = d_q;
+  a.qstride = h->dim;
+  a.nq = nq;
+  a.Ks = d_K;
+  a.Ls = d_L;
+  a.K0 = K0;
+  a.L0 = L0;
+  a.out_off = d_off;
+  a.ids = d_ids;
+  a.dists = d_dists;
+  a.ndc = d_ndc;
+  a.hops = d_hops;
+  a.status = c->status.as<int32_t>();
+  a.work_counter = persistent ? c->counter.as<uint32_t>() : nullptr;
+  a.spill_bits = c->spill.as<uint32_t>();
+  a.spill_words = spill_words(h);
+  a.max_hops = h->n + 1;
+  if (persistent) SS_CUDA(h, cudaMemsetAsync(c->counter.p, 0, 4, stream), "counter reset");
+  SS_CUDA(h, cudaMemsetAsync(c->status.p, 0, (size_t)nq * 4, stream), "status reset");
+  SS_CUDA(h, ssb::launch_warp_search(g, a, plan, wpb, blocks, stream), "search launch");
+  return SS_OK;
+}
+
+int launch_intra(ss_index *h, SearchCtx *c, const float *d_q, uint32_t nq, int K, int L, int W,
+                 uint32_t *d_ids, float *d_dists, uint32_t *d_ndc, uint32_t *d_hops,
+                 cudaStream_t stream) {
+  ssb::GraphView g = h->view();
+  ssb::SmemPlan plan = ssb::plan_intra_smem(g, L, W, h->hash_cap_override);
+  if ((size_t)plan.words_per_team * 4 > 227 * 1024)
+    return set_err(h, SS_ERR_UNSUPPORTED, "L=%d with %d warps needs %u bytes of shared memory",
+                   L, W, plan.words_per_team * 4);
+  SS_CUDA(h, c->spill.ensure((size_t)std::max(nq, 1u) * spill_words(h) * 4, true),
+          "spill bitset allocation");
+  SS_CUDA(h, c->status.ensure((size_t)std::max(nq, 1u) * 4), "status allocation");
+  ssb::BatchArgs a{};
+  a.queries = d_q;
+  a.qstride = h->dim;
+  a.nq = nq;
+  a.K0 = K;
+  a.L0 = L;
+  a.ids = d_ids;
+  a.dists = d_dists;
+  a.ndc = d_ndc;
+  a.hops = d_hops;
+  a.status = c->status.as<int32_t>();
+  a.spill_bits = c->spill.as<uint32_t>();
+  a.spill_words = spill_words(h);
+  a.max_hops = h->n + 1;
+  SS_CUDA(h, cudaMemsetAsync(c->status.p, 0, (size_t)nq * 4, stream), "status reset");
+  SS_CUDA(h, ssb::launch_intra_search(g, a, plan, W, stream), "intra search launch");
+  return SS_OK;
+}
+
+int upload_graph(ss_index *h, const std::vector<uint32_t> &adj, uint32_t rstride, uint32_t ep,
+                 uint32_t max_deg) {
+  DeviceGuard dg(h->device);
+  SS_CUDA(h, h->adj.ensure(adj.size() * 4), "adjacency allocation");
+  SS_CUDA(h, cudaMemcpy(h->adj.p, adj.data(), adj.size() * 4, cudaMemcpyHostToDevice),
+          "adjacency upload");
+  h->rstride = rstride;
+  h->ep = ep;
+  h->max_deg = max_deg;
+  h->has_graph = true;
+  return SS_OK;
+}
+
+int create_common(uint32_t dim, uint32_t num, const float *src, bool src_on_device, int metric,
+                  int device, ss_index **out) {
+  if (!out) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null output handle");
+  *out = nullptr;
+  if (dim == 0 || num == 0 || !src)
+    return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "dim, num and base must be nonzero");
+  if (num >= 0x80000000u) return fail(nullptr, SS_ERR_UNSUPPORTED, "num must be < 2^31");
+  if (metric != SS_METRIC_L2 && metric != SS_METRIC_INNER_PRODUCT)
+    return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "unknown metric %d", metric);
+  int dev = device;
+  if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0)
+    return fail(nullptr, SS_ERR_CUDA, "no CUDA device: %s", cudaGetErrorString(e));
+  if (dev >= ndev) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "device %d out of range", dev);
+  auto h = std::make_unique<ss_index>();
+  h->device = dev;
+  h->dim = dim;
+  h->n = num;
+  h->nb = (dim + 7) / 8;
+  h->metric = metric;
+  DeviceGuard dg(dev);
+  cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, dev);
+  const size_t pitch = (size_t)h->nb * 8 * 4;
+  e = h->base.ensure(pitch * num);
+  if (e != cudaSuccess)
+    return fail(nullptr, SS_ERR_OUT_OF_MEMORY, "base allocation (%zu bytes): %s", pitch * num,
+                cudaGetErrorString(e));
+  if (pitch != (size_t)dim * 4) {
+    e = cudaMemset(h->base.p, 0, pitch * num);
+    if (e != cudaSuccess) return fail(nullptr, SS_ERR_CUDA, "base clear: %s", cudaGetErrorString(e));
+  }
+  e = cudaMemcpy2D(h->base.p, pitch, src, (size_t)dim * 4, (size_t)dim * 4, num,
+                   src_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return fail(nullptr, SS_ERR_CUDA, "base upload: %s", cudaGetErrorString(e));
+  e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return fail(nullptr, SS_ERR_CUDA, "base upload: %s", cudaGetErrorString(e));
+  *out = h.release();
+  return SS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *ss_version(void) { return "scattersearch_b200 0.1 sm_100a"; }
+
+const char *ss_last_error(const ss_index *h) {
+  if (!h) return tl_error.c_str();
+  auto *hh = const_cast<ss_index *>(h);
+  std::lock_guard<std::mutex> lk(hh->mu);
+  tl_handle_error_copy = hh->err;
+  return tl_handle_error_copy.c_str();
+}
+
+void ss_free(void *p) { free(p); }
+
+int ss_create(uint32_t dim, uint32_t num, const float *base_host, int metric, int device,
+              ss_index **out) {
+  return create_common(dim, num, base_host, false, metric, device, out);
+}
+
+int ss_create_from_device(uint32_t dim, uint32_t num, const float *base_dev, int metric,
+                          int device, ss_index **out) {
+  return create_common(dim, num, base_dev, true, metric, device, out);
+}
+
+void ss_destroy(ss_index *h) {
+  if (!h) return;
+  DeviceGuard dg(h->device);
+  cudaDeviceSynchronize();
+  delete h;
+}
+
+int ss_set_graph(ss_index *h, const uint32_t *adj, uint32_t n, uint32_t rstride,
+                 uint32_t entry_point) {
+  if (!h) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null index handle");
+  if (!adj || rstride == 0) return set_err(h, SS_ERR_INVALID_ARGUMENT, "empty adjacency");
+  if (n != h->n) return set_err(h, SS_ERR_FORMAT, "graph has %u nodes, index has %u", n, h->n);
+  if (entry_point >= n)
+    return set_err(h, SS_ERR_FORMAT, "entry point %u out of range (n=%u)", entry_point, n);
+  uint32_t max_deg = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const uint32_t *row = adj + (size_t)i * rstride;
+    uint32_t d = 0;
+    while (d < rstride && row[d] != ssb::kNoneId) {
+      if (row[d] >= n)
+        return set_err(h, SS_ERR_FORMAT, "node %u has neighbour id %u >= n", i, row[d]);
+      ++d;
+    }
+    for (uint32_t m = d; m < rstride; ++m)
+      if (row[m] != ssb::kNoneId)
+        return set_err(h, SS_ERR_FORMAT, "node %u: padding must only follow the neighbours", i);
+    max_deg = std::max(max_deg, d);
+  }
+  if (max_deg > SS_MAX_DEGREE)
+    return set_err(h, SS_ERR_UNSUPPORTED, "degree %u exceeds SS_MAX_DEGREE=%d", max_deg,
+                   SS_MAX_DEGREE);
+  const uint32_t rs = std::max(8u, round_up(max_deg, 8));
+  std::vector<uint32_t> packed((size_t)n * rs, ssb::kNoneId);
+  for (uint32_t i = 0; i < n; ++i)
+    memcpy(&packed[(size_t)i * rs], adj + (size_t)i * rstride, std::min(rs, rstride) * 4);
+  return upload_graph(h, packed, rs, entry_point, max_deg);
+}
+
+int ss_load_graph(ss_index *h, const char *path) {
+  if (!h) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null index handle");
+  if (!path) return set_err(h, SS_ERR_INVALID_ARGUMENT, "null path");
+  FILE *f = fopen(path, "rb");
+  if (!f) return set_err(h, SS_ERR_IO, "cannot open graph file %s", path);
+  uint32_t hdr[2];
+  if (fread(hdr, 4, 2, f) != 2) {
+    fclose(f);
+    return set_err(h, SS_ERR_FORMAT, "%s: missing NSG header", path);
+  }
+  const uint32_t ep = hdr[1];
+  std::vector<std::vector<uint32_t>> rows;
+  rows.reserve(h->n);
+  uint32_t max_deg = 0;
+  for (;;) {
+    uint32_t k;
+    const size_t got = fread(&k, 4, 1, f);
+    if (got != 1) break;  // end of file between records
+    if (k > SS_MAX_DEGREE) {
+      fclose(f);
+      return set_err(h, SS_ERR_UNSUPPORTED, "%s: node %zu has degree %u > SS_MAX_DEGREE", path,
+                     rows.size(), k);
+    }
+    std::vector<uint32_t> r(k);
+    if (k && fread(r.data(), 4, k, f) != k) {
+      fclose(f);
+      return set_err(h, SS_ERR_FORMAT, "%s: truncated record for node %zu", path, rows.size());
+    }
+    max_deg = std::max(max_deg, k);
+    rows.push_back(std::move(r));
+    if (rows.size() > h->n) break;
+  }
+  fclose(f);
+  if (rows.size() != h->n)
+    return set_err(h, SS_ERR_FORMAT, "%s: %zu node records, index has %u", path, rows.size(), h->n);
+  if (ep >= h->n) return set_err(h, SS_ERR_FORMAT, "%s: entry point %u out of range", path, ep);
+  const uint32_t rs = std::max(8u, round_up(max_deg, 8));
+  std::vector<uint32_t> packed((size_t)h->n * rs, ssb::kNoneId);
+  for (uint32_t i = 0; i < h->n; ++i) {
+    for (size_t m = 0; m < rows[i].size(); ++m) {
+      if (rows[i][m] >= h->n)
+        return set_err(h, SS_ERR_FORMAT, "%s: node %u has neighbour id %u >= n", path, i,
+                       rows[i][m]);
+      packed[(size_t)i * rs + m] = rows[i][m];
+    }
+  }
+  return upload_graph(h, packed, rs, ep, max_deg);
+}
+
+int ss_graph_info(const ss_index *h, uint32_t *n, uint32_t *max_degree, uint32_t *entry_point,
+                  uint32_t *rstride) {
+  if (!h) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null index handle");
+  if (n) *n = h->n;
+  if (max_degree) *max_degree = h->max_deg;
+  if (entry_point) *entry_point = h->ep;
+  if (rstride) *rstride = h->rstride;
+  return h->has_graph ? SS_OK : SS_ERR_NO_GRAPH;
+}
+
+int ss_get_graph(ss_index *h, uint32_t *adj, uint32_t rstride) {
+  if (!h) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null index handle");
+  if (!h->has_graph) return set_err(h, SS_ERR_NO_GRAPH, "no graph loaded");
+  if (!adj || rstride < h->max_deg)
+    return set_err(h, SS_ERR_INVALID_ARGUMENT, "rstride %u below max degree %u", rstride,
+                   h->max_deg);
+  DeviceGuard dg(h->device);
+  std::vector<uint32_t> tmp((size_t)h->n * h->rstride);
+  SS_CUDA(h, cudaMemcpy(tmp.data(), h->adj.p, tmp.size() * 4, cudaMemcpyDeviceToHost),
+          "adjacency download");
+  for (uint32_t i = 0; i < h->n; ++i)
+    for (uint32_t m = 0; m < rstride; ++m)
+      adj[(size_t)i * rstride + m] = m < h->rstride ? tmp[(size_t)i * h->rstride + m] : ssb::kNoneId;
+  return SS_OK;
+}
+
+int ss_search(ss_index *h, const float *query, int K, int L, uint32_t *ids, float *dists) {
+  int rc = check_search_args(h, K, L);
+  if (rc) return rc;
+  if (!query || !ids) return set_err(h, SS_ERR_INVALID_ARGUMENT, "null query or ids");
+  DeviceGuard dg(h->device);
+  CtxLease lease(h);
+  SearchCtx *c = lease.c;
+  if (!c) return set_err(h, SS_ERR_CUDA, "cannot create a stream");
+  SS_CUDA(h, c->q.ensure((size_t)h->dim * 4), "query buffer");
+  SS_CUDA(h, c->ids.ensure((size_t)K * 4), "ids buffer");
+  SS_CUDA(h, c->dists.ensure((size_t)K * 4), "dists buffer");
+  SS_CUDA(h, cudaMemcpyAsync(c->q.p, query, (size_t)h->dim * 4, cudaMemcpyHostToDevice, c->stream),
+          "query upload");
+  rc = launch_batch(h, c, c->q.as<float>(), 1, nullptr, nullptr, nullptr, K, L, L,
+                    c->ids.as<uint32_t>(), c->dists.as<float>(), nullptr, nullptr, c->stream, false);
+  if (rc) return rc;
+  int32_t st = 0;
+  SS_CUDA(h, cudaMemcpyAsync(ids, c->ids.p, (size_t)K * 4, cudaMemcpyDeviceToHost, c->stream),
+          "ids download");
+  if (dists)
+    SS_CUDA(h, cudaMemcpyAsync(dists, c->dists.p, (size_t)K * 4, cudaMemcpyDeviceToHost, c->stream),
+            "dists download");
+  SS_CUDA(h, cudaMemcpyAsync(&st, c->status.p, 4, cudaMemcpyDeviceToHost, c->stream),
+          "status download");
+  SS_CUDA(h, cudaStreamSynchronize(c->stream), "search");
+  return status_to_error(h, &st, 1);
+}
+
+static int batch_common(ss_index *h, const float *queries, uint32_t nq, const int32_t *Ks,
+                        const int32_t *Ls, int K, int L, uint32_t *ids, float *dists) {
+  if (!h) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null index handle");
+  if (!h->has_graph) return set_err(h, SS_ERR_NO_GRAPH, "no graph loaded");
+  if (nq == 0) return SS_OK;
+  if (!queries || !ids) return set_err(h, SS_ERR_INVALID_ARGUMENT, "null queries or ids");
+  int L_max = L;
+  size_t total = (size_t)nq * (size_t)K;
+  std::vector<int64_t> off;
+  if (Ks) {
+    L_max = 0;
+    total = 0;
+    off.resize(nq);
+    for (uint32_t i = 0; i < nq; ++i) {
+      int rc = check_search_args(h, Ks[i], Ls[i]);
+      if (rc) return rc;
+      off[i] = (int64_t)total;
+      total += (size_t)Ks[i];
+      L_max = std::max(L_max, (int)Ls[i]);
+    }
+  } else {
+    int rc = check_search_args(h, K, L);
+    if (rc) return rc;
+  }
+  DeviceGuard dg(h->device);
+  CtxLease lease(h);
+  SearchCtx *c = lease.c;
+  if (!c) return set_err(h, SS_ERR_CUDA, "cannot create a stream");
+  SS_CUDA(h, c->q.ensure((size_t)nq * h->dim * 4), "query buffer");
+  SS_CUDA(h, c->ids.ensure(total * 4), "ids buffer");
+  SS_CUDA(h, c->dists.ensure(total * 4), "dists buffer");
+  SS_CUDA(h, cudaMemcpyAsync(c->q.p, queries, (size_t)nq * h->dim * 4, cudaMemcpyHostToDevice,
+                             c->stream),
+          "query upload");
+  if (Ks) {
+    SS_CUDA(h, c->Ks.ensure((size_t)nq * 4), "K buffer");
+    SS_CUDA(h, c->Ls.ensure((size_t)nq * 4), "L buffer");
+    SS_CUDA(h, c->off.ensure((size_t)nq * 8), "offset buffer");
+    SS_CUDA(h, cudaMemcpyAsync(c->Ks.p, Ks, (size_t)nq * 4, cudaMemcpyHostToDevice, c->stream), "K upload");
+    SS_CUDA(h, cudaMemcpyAsync(c->Ls.p, Ls, (size_t)nq * 4, cudaMemcpyHostToDevice, c->stream), "L upload");
+    SS_CUDA(h, cudaMemcpyAsync(c->off.p, off.data(), (size_t)nq * 8, cudaMemcpyHostToDevice, c->stream),
+            "offset upload");
+  }
+  int rc = launch_batch(h, c, c->q.as<float>(), nq, Ks ? c->Ks.as<int32_t>() : nullptr,
+                        Ks ? c->Ls.as<int32_t>() : nullptr, Ks ? c->off.as<int64_t>() : nullptr,
+                        K, L, L_max, c->ids.as<uint32_t>(), c->dists.as<float>(), nullptr, nullptr,
+                        c->stream, true);
+  if (rc) return rc;
+  c->h_status.resize(nq);
+  SS_CUDA(h, cudaMemcpyAsync(ids, c->ids.p, total * 4, cudaMemcpyDeviceToHost, c->stream),
+          "ids download");
+  if (dists)
+    SS_CUDA(h, cudaMemcpyAsync(dists, c->dists.p, total * 4, cudaMemcpyDeviceToHost, c->stream),
+            "dists download");
+  SS_CUDA(h, cudaMemcpyAsync(c->h_status.data(), c->status.p, (size_t)nq * 4,
+                             cudaMemcpyDeviceToHost, c->stream),
+          "status download");
+  SS_CUDA(h, cudaStreamSynchronize(c->stream), "batched search");
+  return status_to_error(h, c->h_status.data(), nq);
+}
+
+int ss_search_batch(ss_index *h, const float *queries, uint32_t nq, int K, int L, uint32_t *ids,
+                    float *dists) {
+  return batch_common(h, queries, nq, nullptr, nullptr, K, L, ids, dists);
+}
+
+int ss_search_batch_uneven(ss_index *h, const float *queries, uint32_t nq, const int32_t *Ks,
+                           const int32_t *Ls, uint32_t *ids, float *dists) {
+  if (!Ks || !Ls) return set_err(h, SS_ERR_INVALID_ARGUMENT, "null Ks or Ls");
+  return batch_common(h, queries, nq, Ks, Ls, 0, 0, ids, dists);
+}
+
+int ss_search_batch_device(ss_index *h, const float *queries, uint32_t nq, const int32_t *Ks,
+                           const int32_t *Ls, const int64_t *out_off, int K, int L, int L_max,
+                           uint32_t *ids, float *dists, uint32_t *ndc, uint32_t *hops,
+                           void *stream) {
+  if (!h) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null index handle");
+  if (!h->has_graph) return set_err(h, SS_ERR_NO_GRAPH, "no graph loaded");
+  if (!queries || !ids) return set_err(h, SS_ERR_INVALID_ARGUMENT, "null queries or ids");
+  const bool uneven = Ks != nullptr;
+  if (uneven != (Ls != nullptr) || uneven != (out_off != nullptr))
+    return set_err(h, SS_ERR_INVALID_ARGUMENT, "Ks, Ls and out_off must be given together");
+  if (uneven) {
+    if (L_max < 1 || L_max > SS_MAX_L)
+      return set_err(h, SS_ERR_INVALID_ARGUMENT, "L_max=%d out of range", L_max);
+  } else {
+    int rc = check_search_args(h, K, L);
+    if (rc) return rc;
+    L_max = L;
+  }
+  DeviceGuard dg(h->device);
+  std::lock_guard<std::mutex> lk(h->dev_mu);
+  h->dev_last_nq = nq;
+  if (nq == 0) return SS_OK;
+  return launch_batch(h, &h->dev_ctx, queries, nq, Ks, Ls, out_off, K, L, L_max, ids, dists, ndc,
+                      hops, static_cast<cudaStream_t>(stream), true);
+}
+
+int ss_batch_status(ss_index *h, uint32_t *failed_queries) {
+  if (!h || !failed_queries) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null argument");
+  DeviceGuard dg(h->device);
+  std::lock_guard<std::mutex> lk(h->dev_mu);
+  const uint32_t nq = h->dev_last_nq;
+  *failed_queries = 0;
+  if (nq == 0) return SS_OK;
+  std::vector<int32_t> st(nq);
+  SS_CUDA(h, cudaMemcpy(st.data(), h->dev_ctx.status.p, (size_t)nq * 4, cudaMemcpyDeviceToHost),
+          "status download");
+  for (uint32_t i = 0; i < nq; ++i) *failed_queries += st[i] != 0;
+  return SS_OK;
+}
+
+static int intra_common(ss_index *h, const float *queries, uint32_t nq, int K, int L, int W,
+                        uint32_t *ids, float *dists) {
+  int rc = check_search_args(h, K, L);
+  if (rc) return rc;
+  if (W < 1 || W > SS_MAX_INTRA_WIDTH)
+    return set_err(h, SS_ERR_INVALID_ARGUMENT, "num_threads=%d outside 1..%d", W,
+                   SS_MAX_INTRA_WIDTH);
+  if (nq == 0) return SS_OK;
+  if (!queries || !ids) return set_err(h, SS_ERR_INVALID_ARGUMENT, "null queries or ids");
+  DeviceGuard dg(h->device);
+  CtxLease lease(h);
+  SearchCtx *c = lease.c;
+  if (!c) return set_err(h, SS_ERR_CUDA, "cannot create a stream");
+  const size_t total = (size_t)nq * K;
+  SS_CUDA(h, c->q.ensure((size_t)nq * h->dim * 4), "query buffer");
+  SS_CUDA(h, c->ids.ensure(total * 4), "ids buffer");
+  SS_CUDA(h, c->dists.ensure(total * 4), "dists buffer");
+  SS_CUDA(h, cudaMemcpyAsync(c->q.p, queries, (size_t)nq * h->dim * 4, cudaMemcpyHostToDevice,
+                             c->stream),
+          "query upload");
+  rc = launch_intra(h, c, c->q.as<float>(), nq, K, L, W, c->ids.as<uint32_t>(),
+                    c->dists.as<float>(), nullptr, nullptr, c->stream);
+  if (rc) return rc;
+  c->h_status.resize(nq);
+  SS_CUDA(h, cudaMemcpyAsync(ids, c->ids.p, total * 4, cudaMemcpyDeviceToHost, c->stream),
+          "ids download");
+  if (dists)
+    SS_CUDA(h, cudaMemcpyAsync(dists, c->dists.p, total * 4, cudaMemcpyDeviceToHost, c->stream),
+            "dists download");
+  SS_CUDA(h, cudaMemcpyAsync(c->h_status.data(), c->status.p, (size_t)nq * 4,
+                             cudaMemcpyDeviceToHost, c->stream),
+          "status download");
+  SS_CUDA(h, cudaStreamSynchronize(c->stream), "intra-query search");
+  return status_to_error(h, c->h_status.data(), nq);
+}
+
+int ss_search_intra(ss_index *h, const float *query, int K, int L, int num_threads, uint32_t *ids,
+                    float *dists) {
+  return intra_common(h, query, 1, K, L, num_threads, ids, dists);
+}
+
+int ss_search_intra_batch(ss_index *h, const float *queries, uint32_t nq, int K, int L,
+                          int num_threads, uint32_t *ids, float *dists) {
+  return intra_common(h, queries, nq, K, L, num_threads, ids, dists);
+}
+
+int ss_search_intra_batch_device(ss_index *h, const float *queries, uint32_t nq, int K, int L,
+                                 int num_threads, uint32_t *ids, float *dists, uint32_t *ndc,
+                                 uint32_t *hops, void *stream) {
+  int rc = check_search_args(h, K, L);
+  if (rc) return rc;
+  if (num_threads < 1 || num_threads > SS_MAX_INTRA_WIDTH)
+    return set_err(h, SS_ERR_INVALID_ARGUMENT, "num_threads=%d outside 1..%d", num_threads,
+                   SS_MAX_INTRA_WIDTH);
+  if (!queries || !ids) return set_err(h, SS_ERR_INVALID_ARGUMENT, "null queries or ids");
+  DeviceGuard dg(h->device);
+  std::lock_guard<std::mutex> lk(h->dev_mu);
+  h->dev_last_nq = nq;
+  if (nq == 0) return SS_OK;
+  return launch_intra(h, &h->dev_ctx, queries, nq, K, L, num_threads, ids, dists, ndc, hops,
+                      static_cast<cudaStream_t>(stream));
+}
+
+int ss_set_tuning(ss_index *h, int warps_per_block, int hash_cap, int blocks_per_sm_cap) {
+  if (!h) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null index handle");
+  if (warps_per_block < 1 || warps_per_block > 8 || (warps_per_block & (warps_per_block - 1)))
+    return set_err(h, SS_ERR_INVALID_ARGUMENT, "warps_per_block must be 1, 2, 4 or 8");
+  h->warps_per_block = warps_per_block;
+  h->hash_cap_override = hash_cap > 0 ? hash_cap : 0;
+  h->blocks_per_sm_cap = blocks_per_sm_cap > 0 ? blocks_per_sm_cap : 0;
+  return SS_OK;
+}
+
+int ss_load_fbin(const char *path, float **data, uint32_t *num, uint32_t *dim) {
+  if (!path || !data || !num || !dim) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null argument");
+  FILE *f = fopen(path, "rb");
+  if (!f) return fail(nullptr, SS_ERR_IO, "cannot open %s", path);
+  uint32_t hdr[2];
+  if (fread(hdr, 4, 2, f) != 2) {
+    fclose(f);
+    return fail(nullptr, SS_ERR_FORMAT, "%s: missing fbin header", path);
+  }
+  const size_t count = (size_t)hdr[0] * hdr[1];
+  float *buf = static_cast<float *>(malloc((count + 8) * sizeof(float)));
+  if (!buf) {
+    fclose(f);
+    return fail(nullptr, SS_ERR_OUT_OF_MEMORY, "%s: cannot allocate %zu floats", path, count);
+  }
+  memset(buf + count, 0, 8 * sizeof(float));
+  if (fread(buf, 4, count, f) != count) {
+    fclose(f);
+    free(buf);
+    return fail(nullptr, SS_ERR_FORMAT, "%s: file shorter than %u x %u floats", path, hdr[0],
+                hdr[1]);
+  }
+  fclose(f);
+  *data = buf;
+  *num = hdr[0];
+  *dim = hdr[1];
+  return SS_OK;
+}
+
+int ss_load_groundtruth(const char *path, uint32_t **ids, uint32_t *nq, uint32_t *k) {
+  if (!path || !ids || !nq || !k) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null argument");
+  FILE *f = fopen(path, "rb");
+  if (!f) return fail(nullptr, SS_ERR_IO, "cannot open %s", path);
+  uint32_t hdr[2];
+  if (fread(hdr, 4, 2, f) != 2) {
+    fclose(f);
+    return fail(nullptr, SS_ERR_FORMAT, "%s: missing ground-truth header", path);
+  }
+  const size_t count = (size_t)hdr[0] * hdr[1];
+  uint32_t *buf = static_cast<uint32_t *>(malloc(std::max<size_t>(count, 1) * 4));
+  if (!buf) {
+    fclose(f);
+    return fail(nullptr, SS_ERR_OUT_OF_MEMORY, "%s: cannot allocate", path);
+  }
+  if (fread(buf, 4, count, f) != count) {
+    fclose(f);
+    free(buf);
+    return fail(nullptr, SS_ERR_FORMAT, "%s: file shorter than %u x %u ids", path, hdr[0], hdr[1]);
+  }
+  fclose(f);
+  *ids = buf;
+  *nq = hdr[0];
+  *k = hdr[1];
+  return SS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,72 @@
+// Internal interface between the host API (ss_api.cpp) and the search
+// kernels (ss_search.cu).  Not installed; the public surface is
+// include/scattersearch.h.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ssb {
+
+constexpr uint32_t kNoneId = 0xFFFFFFFFu;
+
+// Device view of one index: base rows padded to nb*8 floats, fixed-stride
+// adjacency padded with kNoneId.
+struct GraphView {
+  const float *base;     // n x (nb*8) floats
+  const uint32_t *adj;   // n x rstride
+  uint32_t n, dim, nb, rstride, ep;
+  int metric;            // 0 = L2, 1 = inner product
+};
+
+// One batched launch.  Per-query K/L come from Ks/Ls when non-null, else
+// K0/L0.  Results of query q start at out_off[q] (or q*K0).
+struct BatchArgs {
+  const float *queries;  // nq x qstride floats
+  uint32_t qstride, nq;
+  const int32_t *Ks, *Ls;
+  int32_t K0, L0;
+  const int64_t *out_off;
+  uint32_t *ids;
+  float *dists;          // may be null
+  uint32_t *ndc, *hops;  // may be null
+  int32_t *status;       // nq entries, may be null
+  uint32_t *work_counter;  // persistent work queue head; null = static schedule
+  uint32_t *spill_bits;    // per-slot visited bitsets, spill_words each
+  uint32_t spill_words;
+  uint32_t max_hops;
+};
+
+// Per-team shared-memory plan (sizes in 4-byte words, all multiples of 4).
+struct SmemPlan {
+  uint32_t q_words;     // nb*8
+  uint32_t pool_cap;    // >= max L of the launch, multiple of 32
+  uint32_t cand_cap;    // candidates per step (multiple of 32)
+  uint32_t hash_cap;    // power of two
+  uint32_t hash_log2;
+  uint32_t hash_limit;  // entries before spilling to the global bitset
+  uint32_t step_cap;    // CTA kernel: step-local dedupe table (power of two)
+  uint32_t step_log2;
+  uint32_t words_per_team;
+};
+
+// Query status codes written to BatchArgs::status.
+enum : int32_t { kStatusOk = 0, kStatusBadArgs = 1, kStatusHopLimit = 2, kStatusVisitedFull = 3 };
+
+// Plans shared memory for a warp-per-query launch.
+SmemPlan plan_warp_smem(const GraphView &g, int L_max, int hash_cap_override);
+// Plans shared memory for a CTA-per-query launch with `width` expansion warps.
+SmemPlan plan_intra_smem(const GraphView &g, int L_max, int width, int hash_cap_override);
+
+// Launch helpers.  Return cudaSuccess or the launch error.
+//   warps_per_block: teams per CTA; blocks: grid size (0 = one per team
+//   needed for nq with a static schedule).
+cudaError_t launch_warp_search(const GraphView &g, const BatchArgs &a, const SmemPlan &p,
+                               int warps_per_block, int blocks, cudaStream_t stream);
+cudaError_t launch_intra_search(const GraphView &g, const BatchArgs &a, const SmemPlan &p,
+                                int width, cudaStream_t stream);
+
+// Resident CTAs per SM for the warp kernel with this plan (0 if it cannot run).
+int warp_search_occupancy(const GraphView &g, const SmemPlan &p, int warps_per_block);
+
+}  // namespace ssb

@@ -1,0 +1,1037 @@
+// Graph beam-search kernels for sm_100a.
+//
+// Semantics follow ANNSearch::SearchArraySimulation (src/annsearch.cpp:182-259)
+// in its equivalent batch-merge form; see the per-function comments for the
+// exact rules and their reference lines.  The arithmetic of every distance is
+// the reference's AVX model (src/distance.cpp:19-56, :115-149): 8 lane
+// partials, the odd 8-block first when the padded dimension is 8 mod 16, one
+// rounding per subtract, multiply and add (no FMA), lanes summed left to
+// right.  That makes the GPU results bit-identical to the reference built
+// without fast-math.
+//
+// Two kernels:
+//   warp_search_kernel   one warp owns one query (pool, visited hash and
+//                        candidate buffers in shared memory); a CTA holds
+//                        several independent query teams; teams pull queries
+//                        from a device work counter until the batch is empty
+//                        (persistent) or take them by index (static).
+//   intra_search_kernel  one CTA owns one query; each step expands the W best
+//                        unexplored entries at once, one per warp.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ss_internal.h"
+
+namespace ssb {
+namespace {
+
+constexpr uint32_t kExplored = 0x80000000u;
+constexpr unsigned kFull = 0xFFFFFFFFu;
+constexpr uint64_t kInvalidKey = ~0ull;
+
+// ---------------------------------------------------------------- keys ---
+// Order-preserving map float -> uint32 (ascending).  -0 is folded onto +0 so
+// that equal floats get equal keys.  NaN inputs are not supported.
+__device__ __forceinline__ uint32_t float_to_key(float d) {
+  uint32_t u = __float_as_uint(d);
+  if (u == 0x80000000u) u = 0u;
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float key_to_float(uint32_t k) {
+  const uint32_t u = (k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k;
+  return __uint_as_float(u);
+}
+
+__device__ __forceinline__ uint64_t shfl_xor_u64(uint64_t v, int m) {
+  const uint32_t lo = __shfl_xor_sync(kFull, (uint32_t)v, m);
+  const uint32_t hi = __shfl_xor_sync(kFull, (uint32_t)(v >> 32), m);
+  return ((uint64_t)hi << 32) | lo;
+}
+
+__device__ __forceinline__ float4 ldg_f4(const float4 *p) { return __ldg(p); }
+
+// ----------------------------------------------------------- distances ---
+// Block visiting order of distance.cpp:42-51: with an odd number of 8-blocks
+// the last block comes first, then blocks 0, 1, ...
+__device__ __forceinline__ int block_at(int t, int nb) {
+  return (nb & 1) ? (t == 0 ? nb - 1 : t - 1) : t;
+}
+
+__device__ __forceinline__ void acc_l2(float &a0, float &a1, float &a2, float &a3, float4 q,
+                                       float4 v) {
+  float d;
+  d = __fsub_rn(q.x, v.x); a0 = __fadd_rn(a0, __fmul_rn(d, d));
+  d = __fsub_rn(q.y, v.y); a1 = __fadd_rn(a1, __fmul_rn(d, d));
+  d = __fsub_rn(q.z, v.z); a2 = __fadd_rn(a2, __fmul_rn(d, d));
+  d = __fsub_rn(q.w, v.w); a3 = __fadd_rn(a3, __fmul_rn(d, d));
+}
+__device__ __forceinline__ void acc_ip(float &a0, float &a1, float &a2, float &a3, float4 q,
+                                       float4 v) {
+  a0 = __fadd_rn(a0, __fmul_rn(q.x, v.x));
+  a1 = __fadd_rn(a1, __fmul_rn(q.y, v.y));
+  a2 = __fadd_rn(a2, __fmul_rn(q.z, v.z));
+  a3 = __fadd_rn(a3, __fmul_rn(q.w, v.w));
+}
+
+// Distance between the shared-memory query and base row `id`, computed by a
+// lane pair: lane h (0/1) of the pair owns reference lanes 4h..4h+3 and loads
+// one float4 per 8-block.  Both lanes of the pair return the full distance.
+// All 32 lanes must call this (it shuffles); `act` false lanes load nothing.
+template <int NB>
+__device__ __forceinline__ float pair_distance(const GraphView &g, const float *qs, uint32_t id,
+                                               bool act, int h) {
+  const int nb = NB > 0 ? NB : (int)g.nb;
+  const float4 *row = reinterpret_cast<const float4 *>(g.base + (size_t)id * (size_t)(nb * 8)) + h;
+  const float4 *q4 = reinterpret_cast<const float4 *>(qs) + h;
+  float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+  const bool l2 = g.metric == 0;
+  if constexpr (NB > 0) {
+    float4 v[NB];
+#pragma unroll
+    for (int t = 0; t < NB; ++t) {
+      v[t] = act ? ldg_f4(row + 2 * block_at(t, NB)) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    if (l2) {
+#pragma unroll
+      for (int t = 0; t < NB; ++t) acc_l2(a0, a1, a2, a3, q4[2 * block_at(t, NB)], v[t]);
+    } else {
+#pragma unroll
+      for (int t = 0; t < NB; ++t) acc_ip(a0, a1, a2, a3, q4[2 * block_at(t, NB)], v[t]);
+    }
+  } else {
+    for (int t0 = 0; t0 < nb; t0 += 8) {
+      float4 v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int t = t0 + u;
+        v[u] = (act && t < nb) ? ldg_f4(row + 2 * block_at(t, nb)) : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int t = t0 + u;
+        if (t < nb) {
+          if (l2) acc_l2(a0, a1, a2, a3, q4[2 * block_at(t, nb)], v[u]);
+          else acc_ip(a0, a1, a2, a3, q4[2 * block_at(t, nb)], v[u]);
+        }
+      }
+    }
+  }
+  // Horizontal sum u0 + u1 + ... + u7, left to right (distance.cpp:53).
+  const float o0 = __shfl_xor_sync(kFull, a0, 1);
+  const float o1 = __shfl_xor_sync(kFull, a1, 1);
+  const float o2 = __shfl_xor_sync(kFull, a2, 1);
+  const float o3 = __shfl_xor_sync(kFull, a3, 1);
+  const float l0 = h ? o0 : a0, l1 = h ? o1 : a1, l2v = h ? o2 : a2, l3 = h ? o3 : a3;
+  const float u0 = h ? a0 : o0, u1 = h ? a1 : o1, u2 = h ? a2 : o2, u3 = h ? a3 : o3;
+  float r = __fadd_rn(l0, l1);
+  r = __fadd_rn(r, l2v);
+  r = __fadd_rn(r, l3);
+  r = __fadd_rn(r, u0);
+  r = __fadd_rn(r, u1);
+  r = __fadd_rn(r, u2);
+  r = __fadd_rn(r, u3);
+  return l2 ? r : -r;
+}
+
+// Keys of cand_id[0..nc) into cand_key[0..nc); 16 candidates per pass.
+template <int NB>
+__device__ __forceinline__ void eval_candidates(const GraphView &g, const float *qs,
+                                                const uint32_t *cand_id, uint32_t *cand_key, int nc,
+                                                int lane) {
+  const int h = lane & 1;
+  for (int p = 0; p < nc; p += 16) {
+    const int j = p + (lane >> 1);
+    const bool act = j < nc;
+    const uint32_t id = act ? cand_id[j] : 0u;
+    const float d = pair_distance<NB>(g, qs, id, act, h);
+    if (act && h == 0) cand_key[j] = float_to_key(d);
+  }
+}
+
+// -------------------------------------------------------------- sorting ---
+// Ascending bitonic sort of 32*ITEMS 64-bit keys held one per lane per item;
+// element index e = item*32 + lane.
+template <int ITEMS>
+__device__ __forceinline__ void warp_sort(uint64_t (&x)[ITEMS], int lane) {
+  constexpr int N = 32 * ITEMS;
+#pragma unroll
+  for (int k = 2; k <= N; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j >= 32) {
+        const int js = j >> 5;
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i) {
+          const int pi = i ^ js;
+          if (pi > i) {
+            const bool up = ((i * 32 + lane) & k) == 0;
+            const uint64_t a = x[i], b = x[pi];
+            if ((a > b) == up) {
+              x[i] = b;
+              x[pi] = a;
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i) {
+          const uint64_t o = shfl_xor_u64(x[i], j);
+          const bool up = ((i * 32 + lane) & k) == 0;
+          const bool lower = (lane & j) == 0;
+          x[i] = (lower == up) ? (x[i] < o ? x[i] : o) : (x[i] < o ? o : x[i]);
+        }
+      }
+    }
+  }
+}
+
+// Number of a[0..n) with a[i] <= key (a ascending).
+__device__ __forceinline__ int count_le(const uint32_t *a, int n, uint32_t key) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (a[mid] <= key) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+// Number of a[0..n) with a[i] < key (a ascending).
+__device__ __forceinline__ int count_lt(const uint32_t *a, int n, uint32_t key) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (a[mid] < key) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// --------------------------------------------------------- visited set ---
+// Exact visited set: open-addressing hash of ids in shared memory (linear
+// probing).  When it reaches `limit` entries, further ids go to a per-team
+// bitset in global memory (n bits), so nothing is ever forgotten; lookups
+// then check both.  The bitset is cleared again before the team's next query.
+struct Visited {
+  uint32_t *tab;
+  uint32_t mask, log2cap, limit, count;
+  uint32_t *bits;  // global, may be null when spilling is impossible
+  bool spilled;
+};
+
+__device__ __forceinline__ uint32_t hash_slot(uint32_t id, uint32_t log2cap) {
+  return (id * 0x9E3779B1u) >> (32 - log2cap);
+}
+
+// Inserts `id`; true if it was not present.  Distinct lanes may race on the
+// same id: the atomicCAS lets exactly one of them see it as new.
+__device__ __forceinline__ bool hash_insert(uint32_t *tab, uint32_t mask, uint32_t log2cap,
+                                            uint32_t id) {
+  uint32_t s = hash_slot(id, log2cap);
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    const uint32_t cur = tab[s];
+    if (cur == id) return false;
+    if (cur == kNoneId) {
+      const uint32_t old = atomicCAS(&tab[s], kNoneId, id);
+      if (old == kNoneId) return true;
+      if (old == id) return false;
+    }
+    s = (s + 1) & mask;
+  }
+  return false;  // unreachable: the table never fills past `limit`
+}
+
+__device__ __forceinline__ bool hash_contains(const uint32_t *tab, uint32_t mask, uint32_t log2cap,
+                                              uint32_t id) {
+  uint32_t s = hash_slot(id, log2cap);
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    const uint32_t cur = tab[s];
+    if (cur == id) return true;
+    if (cur == kNoneId) return false;
+    s = (s + 1) & mask;
+  }
+  return false;
+}
+
+// Marks `id` visited; true if it was new.
+__device__ __forceinline__ bool visit(Visited &v, uint32_t id) {
+  if (!v.spilled) return hash_insert(v.tab, v.mask, v.log2cap, id);
+  if (hash_contains(v.tab, v.mask, v.log2cap, id)) return false;
+  const uint32_t bit = 1u << (id & 31u);
+  return (atomicOr(v.bits + (id >> 5), bit) & bit) == 0u;
+}
+
+// Read-only membership test.
+__device__ __forceinline__ bool visited_test(const Visited &v, uint32_t id) {
+  if (hash_contains(v.tab, v.mask, v.log2cap, id)) return true;
+  if (!v.spilled) return false;
+  const uint32_t bit = 1u << (id & 31u);
+  return (*(volatile uint32_t *)(v.bits + (id >> 5)) & bit) != 0u;
+}
+
+// ------------------------------------------------------- warp per query ---
+struct WarpSmem {
+  float *q;
+  uint32_t *pk, *pid;          // pool keys / ids (bit 31 of id = explored)
+  uint32_t *cand_id, *cand_key, *sk;
+  uint32_t *hash;
+};
+
+__device__ __forceinline__ WarpSmem carve_warp(uint32_t *base, const SmemPlan &p) {
+  WarpSmem s;
+  s.q = reinterpret_cast<float *>(base);
+  base += p.q_words;
+  s.pk = base;
+  base += p.pool_cap;
+  s.pid = base;
+  base += p.pool_cap;
+  s.cand_id = base;
+  base += p.cand_cap;
+  s.cand_key = base;
+  base += p.cand_cap;
+  s.sk = base;
+  base += p.cand_cap;
+  s.hash = base;
+  return s;
+}
+
+// One query, one warp.  Steps per hop (batch-merge form of
+// annsearch.cpp:218-253):
+//   1. expand the first unexplored pool slot (all slots before `cursor` are
+//      explored);
+//   2. read its adjacency row; drop ids already visited and mark the rest
+//      visited, the first occurrence in adjacency order winning (:229-231);
+//   3. compute their distances (:236);
+//   4. accept d < pool[size-1] taken at the start of the hop (:238);
+//   5. sort accepted candidates by (d, adjacency position) and stable-merge
+//      them into the pool, older entries first on ties, truncated to L
+//      (InsertIntoPool upper-bound insert, util.h:56-75; :242-243).
+template <int NB, int RCH>
+__device__ void warp_search_one(const GraphView &g, const float *__restrict__ qsrc, int K, int L,
+                                uint32_t *out_ids, float *out_dists, uint32_t *out_ndc,
+                                uint32_t *out_hops, int32_t *out_status, const WarpSmem &s,
+                                const SmemPlan &p, uint32_t *spill, uint32_t spill_words,
+                                uint32_t max_hops, int lane) {
+  const unsigned lanemask_lt = (1u << lane) - 1u;
+  const int qw = (int)g.nb * 8;
+  for (int i = lane; i < qw; i += 32) s.q[i] = i < (int)g.dim ? qsrc[i] : 0.f;
+  for (uint32_t i = lane; i < p.hash_cap; i += 32) s.hash[i] = kNoneId;
+  __syncwarp();
+
+  Visited vis;
+  vis.tab = s.hash;
+  vis.mask = p.hash_cap - 1;
+  vis.log2cap = p.hash_log2;
+  vis.limit = p.hash_limit;
+  vis.count = 0;
+  vis.bits = spill;
+  vis.spilled = false;
+
+  uint32_t ndc = 0, hops = 0;
+  int32_t status = kStatusOk;
+
+  // Initial pool: the first min(L, deg(ep)) neighbours of the entry point,
+  // all marked visited, sorted by distance (annsearch.cpp:185-215).  Exact
+  // ties keep adjacency order.
+  int size = 0;
+  {
+    const uint32_t *erow = g.adj + (size_t)g.ep * g.rstride;
+#pragma unroll
+    for (int c = 0; c < RCH; ++c) {
+      const int m = c * 32 + lane;
+      const uint32_t id = m < (int)g.rstride ? __ldg(erow + m) : kNoneId;
+      const bool valid = id != kNoneId && m < L;
+      if (valid) {
+        s.cand_id[m] = id;
+        visit(vis, id);
+      }
+      size += __popc(__ballot_sync(kFull, valid));
+    }
+    vis.count = size;
+    __syncwarp();
+    eval_candidates<NB>(g, s.q, s.cand_id, s.cand_key, size, lane);
+    ndc += size;
+    __syncwarp();
+    uint64_t x[RCH];
+#pragma unroll
+    for (int i = 0; i < RCH; ++i) {
+      const int e = i * 32 + lane;
+      x[i] = e < size ? (((uint64_t)s.cand_key[e] << 32) | (uint32_t)e) : kInvalidKey;
+    }
+    warp_sort<RCH>(x, lane);
+#pragma unroll
+    for (int i = 0; i < RCH; ++i) {
+      const int e = i * 32 + lane;
+      if (e < size) {
+        s.pk[e] = (uint32_t)(x[i] >> 32);
+        s.pid[e] = s.cand_id[(uint32_t)x[i]];
+      }
+    }
+    __syncwarp();
+  }
+
+  int cursor = 0;
+  for (;;) {
+    // 1. first unexplored slot at or after the cursor
+    int k = -1;
+    for (int b0 = cursor; b0 < size; b0 += 32) {
+      const int idx = b0 + lane;
+      const bool un = idx < size && !(s.pid[idx] & kExplored);
+      const unsigned bm = __ballot_sync(kFull, un);
+      if (bm) {
+        k = b0 + __ffs(bm) - 1;
+        break;
+      }
+    }
+    if (k < 0) break;
+    if (hops >= max_hops) {
+      status = kStatusHopLimit;
+      break;
+    }
+    const uint32_t node = s.pid[k];
+    const uint32_t thr = s.pk[size - 1];
+    __syncwarp();
+    if (lane == 0) s.pid[k] = node | kExplored;
+    ++hops;
+    cursor = k + 1;
+
+    // 2. adjacency row, in-row dedupe, visited filter, compaction in m order
+    const uint32_t *nrow = g.adj + (size_t)node * g.rstride;
+    int nc = 0;
+#pragma unroll
+    for (int c = 0; c < RCH; ++c) {
+      const int m = c * 32 + lane;
+      const uint32_t id = m < (int)g.rstride ? __ldg(nrow + m) : kNoneId;
+      const bool valid = id != kNoneId;
+      const unsigned peers = __match_any_sync(kFull, id);
+      const bool leader = valid && (peers & lanemask_lt) == 0u;
+      if (!vis.spilled && vis.count + 32u > vis.limit) {
+        if (!spill) {
+          status = kStatusVisitedFull;
+          break;
+        }
+        vis.spilled = true;
+      }
+      const bool fresh = leader && visit(vis, id);
+      const unsigned fm = __ballot_sync(kFull, fresh);
+      if (fresh) s.cand_id[nc + __popc(fm & lanemask_lt)] = id;
+      nc += __popc(fm);
+      if (!vis.spilled) vis.count += __popc(fm);
+    }
+    if (status != kStatusOk) break;
+    if (nc == 0) continue;
+    __syncwarp();
+
+    // 3. distances
+    eval_candidates<NB>(g, s.q, s.cand_id, s.cand_key, nc, lane);
+    ndc += nc;
+    __syncwarp();
+
+    // 4. acceptance + sort by (key, m)
+    uint64_t x[RCH];
+    int na = 0;
+#pragma unroll
+    for (int i = 0; i < RCH; ++i) {
+      const int e = i * 32 + lane;
+      const bool acc = e < nc && s.cand_key[e] < thr;
+      x[i] = acc ? (((uint64_t)s.cand_key[e] << 32) | (uint32_t)e) : kInvalidKey;
+      na += __popc(__ballot_sync(kFull, acc));
+    }
+    if (na == 0) continue;
+    warp_sort<RCH>(x, lane);
+
+    // 5. stable merge into the pool, in place
+    uint32_t nkey[RCH], nid[RCH];
+    int npos[RCH];
+#pragma unroll
+    for (int i = 0; i < RCH; ++i) npos[i] = 0;
+#pragma unroll
+    for (int i = 0; i < RCH; ++i) {
+      const int e = i * 32 + lane;
+      if (e < na) {
+        nkey[i] = (uint32_t)(x[i] >> 32);
+        nid[i] = s.cand_id[(uint32_t)x[i]];
+        s.sk[e] = nkey[i];
+        npos[i] = e + count_le(s.pk, size, nkey[i]);
+      }
+    }
+    const int p0 = __shfl_sync(kFull, npos[0], 0);
+    __syncwarp();
+    // Old entries at and after p0 move up by the number of new keys below
+    // them.  Chunks go from the top down so no entry is overwritten before
+    // it has been read.
+    for (int hi = size; hi > p0; hi -= 32) {
+      const int j = hi - 32 + lane;
+      const bool act = j >= p0;
+      uint32_t ok = 0, oid = 0;
+      int t = 0;
+      if (act) {
+        ok = s.pk[j];
+        oid = s.pid[j];
+        t = j + count_lt(s.sk, na, ok);
+      }
+      __syncwarp();
+      if (act && t < L) {
+        s.pk[t] = ok;
+        s.pid[t] = oid;
+      }
+      __syncwarp();
+    }
+#pragma unroll
+    for (int i = 0; i < RCH; ++i) {
+      const int e = i * 32 + lane;
+      if (e < na && npos[i] < L) {
+        s.pk[npos[i]] = nkey[i];
+        s.pid[npos[i]] = nid[i];
+      }
+    }
+    __syncwarp();
+    size = min(L, size + na);
+    cursor = min(cursor, p0);
+  }
+
+  // Results: slots the pool never filled keep the reference's value-
+  // initialised Neighbor (id 0, distance 0), annsearch.cpp:193, :254-257.
+  for (int i = lane; i < K; i += 32) {
+    const bool have = i < size;
+    out_ids[i] = have ? (s.pid[i] & ~kExplored) : 0u;
+    if (out_dists) out_dists[i] = have ? key_to_float(s.pk[i]) : 0.f;
+  }
+  if (vis.spilled) {
+    for (uint32_t w = lane; w < spill_words; w += 32) spill[w] = 0u;
+  }
+  if (lane == 0) {
+    if (out_ndc) *out_ndc = ndc;
+    if (out_hops) *out_hops = hops;
+    if (out_status) *out_status = status;
+  }
+  __syncwarp();
+}
+
+template <int NB, int RCH>
+__global__ void __launch_bounds__(256) warp_search_kernel(GraphView g, BatchArgs a, SmemPlan p) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  const WarpSmem s = carve_warp(smem + (size_t)warp * p.words_per_team, p);
+  const uint32_t slot = blockIdx.x * wpb + warp;
+  const uint32_t nslots = gridDim.x * wpb;
+  uint32_t *spill = a.spill_bits ? a.spill_bits + (size_t)slot * a.spill_words : nullptr;
+  uint32_t q = slot;
+  for (;;) {
+    if (a.work_counter) {
+      uint32_t t = 0;
+      if (lane == 0) t = atomicAdd(a.work_counter, 1u);
+      q = __shfl_sync(kFull, t, 0);
+    }
+    if (q >= a.nq) break;
+    const int K = a.Ks ? a.Ks[q] : a.K0;
+    const int L = a.Ls ? a.Ls[q] : a.L0;
+    const int64_t off = a.out_off ? a.out_off[q] : (int64_t)q * a.K0;
+    if (K < 1 || K > L || L > (int)p.pool_cap) {
+      if (lane == 0 && a.status) a.status[q] = kStatusBadArgs;
+    } else {
+      warp_search_one<NB, RCH>(g, a.queries + (size_t)q * a.qstride, K, L, a.ids + off,
+                               a.dists ? a.dists + off : nullptr, a.ndc ? a.ndc + q : nullptr,
+                               a.hops ? a.hops + q : nullptr, a.status ? a.status + q : nullptr, s,
+                               p, spill, a.spill_words, a.max_hops, lane);
+    }
+    if (!a.work_counter) q += nslots;
+  }
+}
+
+// ------------------------------------------------------- CTA per query ---
+// W warps share one query.  Each step (the several-candidates-per-step form,
+// structured like ModifiedDeltaStepping, annsearch.cpp:1632-1691, with the
+// acceptance and termination rules of SearchArraySimulation):
+//   A. warp 0 picks the first W unexplored slots; the acceptance threshold is
+//      pool[size-1] at this point;
+//   B. warp w reads the adjacency row of pick w, dedupes it, and keeps ids
+//      that were not visited before this step;
+//   C. ids seen by several warps in the same step are resolved in (w, m)
+//      order through a step-local table with atomicMin claims, so the first
+//      occurrence wins exactly as a sequential scan would;
+//   D. winners are marked visited and evaluated; accepted ones are sorted per
+//      warp by (key, m);
+//   E. the pool and all W sorted lists are merged by rank (ties: old pool,
+//      then lower w, then lower m) into the second pool buffer.
+// With W = 1 this is exactly the warp kernel's search.
+struct CtaSmem {
+  float *q;
+  uint32_t *pk[2], *pid[2];
+  uint32_t *hash;
+  uint32_t *st_id, *st_claim;           // step-local dedupe table
+  uint32_t *wc_id, *wc_key, *wc_slot;   // per-warp candidates [W][cand_cap]
+  uint32_t *ws_key, *ws_id;             // per-warp sorted accepted [W][cand_cap]
+  int *wn;                              // per-warp accepted counts [W]
+  int *misc;                            // [0] npicks, [1..W] picks, [W+1] pmin
+};
+
+constexpr int kStepTableFactor = 2;
+
+__device__ __forceinline__ uint32_t st_find_or_insert(uint32_t *tab, uint32_t mask, uint32_t log2cap,
+                                                      uint32_t id) {
+  uint32_t s = hash_slot(id, log2cap);
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    const uint32_t cur = tab[s];
+    if (cur == id) return s;
+    if (cur == kNoneId) {
+      const uint32_t old = atomicCAS(&tab[s], kNoneId, id);
+      if (old == kNoneId || old == id) return s;
+    }
+    s = (s + 1) & mask;
+  }
+  return 0xFFFFFFFFu;  // unreachable: the table holds twice the step's candidates
+}
+
+template <int NB, int RCH>
+__global__ void __launch_bounds__(512) intra_search_kernel(GraphView g, BatchArgs a, SmemPlan p,
+                                                           int W) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nthr = blockDim.x;
+  const unsigned lanemask_lt = (1u << lane) - 1u;
+  const uint32_t q_idx = blockIdx.x;
+  if (q_idx >= a.nq) return;
+  const int K = a.Ks ? a.Ks[q_idx] : a.K0;
+  const int L = a.Ls ? a.Ls[q_idx] : a.L0;
+  const int64_t off = a.out_off ? a.out_off[q_idx] : (int64_t)q_idx * a.K0;
+  if (K < 1 || K > L || L > (int)p.pool_cap) {
+    if (threadIdx.x == 0 && a.status) a.status[q_idx] = kStatusBadArgs;
+    return;
+  }
+  const int cc = (int)p.cand_cap;
+  const uint32_t st_cap = p.step_cap;
+  const uint32_t st_log2 = p.step_log2;
+
+  CtaSmem s;
+  {
+    uint32_t *b = smem;
+    s.q = reinterpret_cast<float *>(b); b += p.q_words;
+    s.pk[0] = b; b += p.pool_cap;
+    s.pid[0] = b; b += p.pool_cap;
+    s.pk[1] = b; b += p.pool_cap;
+    s.pid[1] = b; b += p.pool_cap;
+    s.hash = b; b += p.hash_cap;
+    s.st_id = b; b += st_cap;
+    s.st_claim = b; b += st_cap;
+    s.wc_id = b; b += W * cc;
+    s.wc_key = b; b += W * cc;
+    s.wc_slot = b; b += W * cc;
+    s.ws_key = b; b += W * cc;
+    s.ws_id = b; b += W * cc;
+    s.wn = reinterpret_cast<int *>(b); b += 32;
+    s.misc = reinterpret_cast<int *>(b);
+  }
+  uint32_t *spill = a.spill_bits ? a.spill_bits + (size_t)q_idx * a.spill_words : nullptr;
+
+  const float *qsrc = a.queries + (size_t)q_idx * a.qstride;
+  const int qw = (int)g.nb * 8;
+  for (int i = threadIdx.x; i < qw; i += nthr) s.q[i] = i < (int)g.dim ? qsrc[i] : 0.f;
+  for (uint32_t i = threadIdx.x; i < p.hash_cap; i += nthr) s.hash[i] = kNoneId;
+  for (uint32_t i = threadIdx.x; i < st_cap; i += nthr) {
+    s.st_id[i] = kNoneId;
+    s.st_claim[i] = 0xFFFFFFFFu;
+  }
+  __syncthreads();
+
+  Visited vis;
+  vis.tab = s.hash;
+  vis.mask = p.hash_cap - 1;
+  vis.log2cap = p.hash_log2;
+  vis.limit = p.hash_limit;
+  vis.count = 0;
+  vis.bits = spill;
+  vis.spilled = false;
+
+  uint32_t ndc = 0, hops = 0;
+  int32_t status = kStatusOk;
+  int cur = 0;  // active pool buffer
+  int size = 0;
+
+  // Initial pool (warp 0), identical to the warp kernel's.
+  if (warp == 0) {
+    const uint32_t *erow = g.adj + (size_t)g.ep * g.rstride;
+    uint32_t *cid = s.wc_id, *ckey = s.wc_key;
+#pragma unroll
+    for (int c = 0; c < RCH; ++c) {
+      const int m = c * 32 + lane;
+      const uint32_t id = m < (int)g.rstride ? __ldg(erow + m) : kNoneId;
+      const bool valid = id != kNoneId && m < L;
+      if (valid) {
+        cid[m] = id;
+        visit(vis, id);
+      }
+      size += __popc(__ballot_sync(kFull, valid));
+    }
+    __syncwarp();
+    eval_candidates<NB>(g, s.q, cid, ckey, size, lane);
+    __syncwarp();
+    uint64_t x[RCH];
+#pragma unroll
+    for (int i = 0; i < RCH; ++i) {
+      const int e = i * 32 + lane;
+      x[i] = e < size ? (((uint64_t)ckey[e] << 32) | (uint32_t)e) : kInvalidKey;
+    }
+    warp_sort<RCH>(x, lane);
+#pragma unroll
+    for (int i = 0; i < RCH; ++i) {
+      const int e = i * 32 + lane;
+      if (e < size) {
+        s.pk[0][e] = (uint32_t)(x[i] >> 32);
+        s.pid[0][e] = cid[(uint32_t)x[i]];
+      }
+    }
+    if (lane == 0) s.misc[0] = size;
+  }
+  __syncthreads();
+  size = s.misc[0];
+  vis.count = size;
+  ndc += size;
+
+  int cursor = 0;
+  for (;;) {
+    uint32_t *pk = s.pk[cur], *pid = s.pid[cur];
+    // A. picks
+    if (warp == 0) {
+      int np = 0, last = -1;
+      for (int b0 = cursor; b0 < size && np < W; b0 += 32) {
+        const int idx = b0 + lane;
+        const bool un = idx < size && !(pid[idx] & kExplored);
+        const unsigned bm = __ballot_sync(kFull, un);
+        if (un) {
+          const int r = np + __popc(bm & lanemask_lt);
+          if (r < W) {
+            s.misc[1 + r] = idx;
+            last = idx;
+          }
+        }
+        np += __popc(bm);
+      }
+      np = min(np, W);
+      // highest picked index: max over lanes of `last`
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) last = max(last, __shfl_xor_sync(kFull, last, o));
+      if (lane == 0) {
+        s.misc[0] = np;
+        s.misc[W + 2] = last;
+      }
+    }
+    __syncthreads();
+    const int np = s.misc[0];
+    if (np == 0) break;
+    if (hops >= a.max_hops) {
+      status = kStatusHopLimit;
+      break;
+    }
+    // Spill decision for this step, identical in every thread: the step can
+    // add at most W * cand_cap entries.
+    if (!vis.spilled && vis.count + (uint32_t)(W * cc) > p.hash_limit) {
+      if (!spill) {
+        status = kStatusVisitedFull;
+        break;
+      }
+      vis.spilled = true;
+    }
+    const uint32_t thr = pk[size - 1];
+    cursor = s.misc[W + 2] + 1;
+    hops += np;
+
+    // B. per-warp adjacency row: in-row dedupe + not-yet-visited filter
+    int nfresh = 0;
+    uint32_t my_node = 0;
+    if (warp < np) {
+      my_node = pid[s.misc[1 + warp]];
+      const uint32_t *nrow = g.adj + (size_t)my_node * g.rstride;
+#pragma unroll
+      for (int c = 0; c < RCH; ++c) {
+        const int m = c * 32 + lane;
+        const uint32_t id = m < (int)g.rstride ? __ldg(nrow + m) : kNoneId;
+        const bool valid = id != kNoneId;
+        const unsigned peers = __match_any_sync(kFull, id);
+        const bool leader = valid && (peers & lanemask_lt) == 0u;
+        const bool fresh = leader && !visited_test(vis, id);
+        const unsigned fm = __ballot_sync(kFull, fresh);
+        if (fresh) {
+          const int pos = nfresh + __popc(fm & lanemask_lt);
+          s.wc_id[warp * cc + pos] = id;
+          // C. claim in (w, m) order
+          const uint32_t slot = st_find_or_insert(s.st_id, st_cap - 1, st_log2, id);
+          s.wc_slot[warp * cc + pos] = slot;
+          atomicMin(&s.st_claim[slot], (uint32_t)(warp * cc + m));
+          s.wc_key[warp * cc + pos] = (uint32_t)m;  // remember m until claims settle
+        }
+        nfresh += __popc(fm);
+      }
+    }
+    __syncthreads();
+    // mark explored (after every warp has read its node id)
+    if (threadIdx.x < (unsigned)np) {
+      const int kk = s.misc[1 + threadIdx.x];
+      pid[kk] |= kExplored;
+    }
+
+    // D. winners: visited insert, distance, acceptance, per-warp sort
+    int nwin = 0;
+    if (warp < np) {
+      for (int c0 = 0; c0 < nfresh; c0 += 32) {
+        const int e = c0 + lane;
+        bool win = false;
+        uint32_t id = 0;
+        if (e < nfresh) {
+          const uint32_t m = s.wc_key[warp * cc + e];
+          const uint32_t slot = s.wc_slot[warp * cc + e];
+          id = s.wc_id[warp * cc + e];
+          win = s.st_claim[slot] == (uint32_t)(warp * cc + (int)m);
+        }
+        const unsigned wm = __ballot_sync(kFull, win);
+        if (win) {
+          visit(vis, id);
+          // compact winners in place (positions only move down)
+          s.ws_id[warp * cc + nwin + __popc(wm & lanemask_lt)] = id;
+        }
+        nwin += __popc(wm);
+      }
+    }
+    // every warp applies the same count update so vis.count stays uniform
+    __syncthreads();
+    if (warp < np && lane == 0) s.wn[warp] = nwin;
+    __syncthreads();
+    {
+      int tot = 0;
+      for (int w = 0; w < np; ++w) tot += s.wn[w];
+      if (!vis.spilled) vis.count += tot;
+      ndc += tot;
+    }
+    // reset the step table slots used this step (claims and ids)
+    if (warp < np) {
+      for (int e = lane; e < nfresh; e += 32) {
+        const uint32_t slot = s.wc_slot[warp * cc + e];
+        s.st_id[slot] = kNoneId;
+        s.st_claim[slot] = 0xFFFFFFFFu;
+      }
+    }
+    int nacc = 0;
+    if (warp < np) {
+      // distances of the winners (ws_id[warp][0..nwin)) into wc_key
+      eval_candidates<NB>(g, s.q, s.ws_id + warp * cc, s.wc_key + warp * cc, nwin, lane);
+      __syncwarp();
+      uint64_t x[RCH];
+#pragma unroll
+      for (int i = 0; i < RCH; ++i) {
+        const int e = i * 32 + lane;
+        const bool acc = e < nwin && s.wc_key[warp * cc + e] < thr;
+        x[i] = acc ? (((uint64_t)s.wc_key[warp * cc + e] << 32) | (uint32_t)e) : kInvalidKey;
+        nacc += __popc(__ballot_sync(kFull, acc));
+      }
+      warp_sort<RCH>(x, lane);
+      uint32_t sid[RCH];
+#pragma unroll
+      for (int i = 0; i < RCH; ++i) {
+        const int e = i * 32 + lane;
+        if (e < nacc) sid[i] = s.ws_id[warp * cc + (uint32_t)x[i]];
+      }
+      __syncwarp();
+#pragma unroll
+      for (int i = 0; i < RCH; ++i) {
+        const int e = i * 32 + lane;
+        if (e < nacc) {
+          s.ws_key[warp * cc + e] = (uint32_t)(x[i] >> 32);
+          s.ws_id[warp * cc + e] = sid[i];
+        }
+      }
+    }
+    __syncthreads();
+    if (warp < np && lane == 0) s.wn[warp] = nacc;
+    __syncthreads();
+    int total = 0;
+    for (int w = 0; w < np; ++w) total += s.wn[w];
+    if (total == 0) continue;
+
+    // E. rank merge into the other buffer
+    uint32_t *npk = s.pk[cur ^ 1], *npid = s.pid[cur ^ 1];
+    if (threadIdx.x == 0) s.misc[W + 1] = 0x7FFFFFFF;
+    __syncthreads();
+    int local_min = 0x7FFFFFFF;
+    // old entries
+    for (int j = threadIdx.x; j < size; j += nthr) {
+      const uint32_t key = pk[j];
+      int t = j;
+      for (int w = 0; w < np; ++w) t += count_lt(s.ws_key + w * cc, s.wn[w], key);
+      if (t < L) {
+        npk[t] = key;
+        npid[t] = pid[j];
+      }
+    }
+    // new entries: list w, element e
+    for (int w = 0; w < np; ++w) {
+      for (int e = threadIdx.x; e < s.wn[w]; e += nthr) {
+        const uint32_t key = s.ws_key[w * cc + e];
+        int t = e + count_le(pk, size, key);
+        for (int v = 0; v < np; ++v) {
+          if (v == w) continue;
+          t += (v < w) ? count_le(s.ws_key + v * cc, s.wn[v], key)
+                       : count_lt(s.ws_key + v * cc, s.wn[v], key);
+        }
+        if (t < L) {
+          npk[t] = key;
+          npid[t] = s.ws_id[w * cc + e];
+        }
+        local_min = min(local_min, t);
+      }
+    }
+    if (local_min != 0x7FFFFFFF) atomicMin(&s.misc[W + 1], local_min);
+    __syncthreads();
+    size = min(L, size + total);
+    cursor = min(cursor, s.misc[W + 1]);
+    cur ^= 1;
+  }
+
+  // results
+  {
+    const uint32_t *pk = s.pk[cur], *pid = s.pid[cur];
+    uint32_t *oid = a.ids + off;
+    float *od = a.dists ? a.dists + off : nullptr;
+    for (int i = threadIdx.x; i < K; i += nthr) {
+      const bool have = i < size;
+      oid[i] = have ? (pid[i] & ~kExplored) : 0u;
+      if (od) od[i] = have ? key_to_float(pk[i]) : 0.f;
+    }
+  }
+  if (vis.spilled && spill) {
+    __syncthreads();
+    for (uint32_t w = threadIdx.x; w < a.spill_words; w += nthr) spill[w] = 0u;
+  }
+  if (threadIdx.x == 0) {
+    if (a.ndc) a.ndc[q_idx] = ndc;
+    if (a.hops) a.hops[q_idx] = hops;
+    if (a.status) a.status[q_idx] = status;
+  }
+}
+
+// ----------------------------------------------------------- dispatch ---
+using WarpFn = void (*)(GraphView, BatchArgs, SmemPlan);
+using IntraFn = void (*)(GraphView, BatchArgs, SmemPlan, int);
+
+template <int RCH>
+WarpFn warp_fn_for_nb(uint32_t nb) {
+  switch (nb) {
+    case 8: return warp_search_kernel<8, RCH>;
+    case 12: return warp_search_kernel<12, RCH>;
+    case 16: return warp_search_kernel<16, RCH>;
+    case 25: return warp_search_kernel<25, RCH>;
+    default: return warp_search_kernel<0, RCH>;
+  }
+}
+template <int RCH>
+IntraFn intra_fn_for_nb(uint32_t nb) {
+  switch (nb) {
+    case 8: return intra_search_kernel<8, RCH>;
+    case 12: return intra_search_kernel<12, RCH>;
+    case 16: return intra_search_kernel<16, RCH>;
+    case 25: return intra_search_kernel<25, RCH>;
+    default: return intra_search_kernel<0, RCH>;
+  }
+}
+
+WarpFn warp_fn(const GraphView &g) {
+  const uint32_t rch = (g.rstride + 31) / 32;
+  if (rch <= 1) return warp_fn_for_nb<1>(g.nb);
+  if (rch <= 2) return warp_fn_for_nb<2>(g.nb);
+  return warp_fn_for_nb<4>(g.nb);
+}
+IntraFn intra_fn(const GraphView &g) {
+  const uint32_t rch = (g.rstride + 31) / 32;
+  if (rch <= 1) return intra_fn_for_nb<1>(g.nb);
+  if (rch <= 2) return intra_fn_for_nb<2>(g.nb);
+  return intra_fn_for_nb<4>(g.nb);
+}
+
+uint32_t round_up(uint32_t x, uint32_t m) { return (x + m - 1) / m * m; }
+uint32_t pow2_at_least(uint32_t x) {
+  uint32_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+uint32_t log2_of(uint32_t p) {
+  uint32_t l = 0;
+  while ((1u << l) < p) ++l;
+  return l;
+}
+
+}  // namespace
+
+SmemPlan plan_warp_smem(const GraphView &g, int L_max, int hash_cap_override) {
+  SmemPlan p{};
+  p.q_words = g.nb * 8;
+  p.pool_cap = round_up((uint32_t)L_max, 32);
+  p.cand_cap = round_up(g.rstride, 32);
+  uint32_t hc = hash_cap_override > 0 ? pow2_at_least((uint32_t)hash_cap_override)
+                                      : pow2_at_least((uint32_t)L_max * 16u);
+  if (hc < 1024) hc = 1024;
+  if (hc > 32768) hc = 32768;
+  p.hash_cap = hc;
+  p.hash_log2 = log2_of(hc);
+  p.hash_limit = hc - hc / 4;  // 75% load, then spill
+  p.words_per_team = p.q_words + 2 * p.pool_cap + 3 * p.cand_cap + p.hash_cap;
+  p.words_per_team = round_up(p.words_per_team, 4);
+  return p;
+}
+
+SmemPlan plan_intra_smem(const GraphView &g, int L_max, int width, int hash_cap_override) {
+  SmemPlan p{};
+  p.q_words = g.nb * 8;
+  p.pool_cap = round_up((uint32_t)L_max, 32);
+  p.cand_cap = round_up(g.rstride, 32);
+  uint32_t hc = hash_cap_override > 0 ? pow2_at_least((uint32_t)hash_cap_override)
+                                      : pow2_at_least((uint32_t)L_max * 16u * (uint32_t)width);
+  if (hc < 1024) hc = 1024;
+  if (hc > 16384) hc = 16384;
+  p.hash_cap = hc;
+  p.hash_log2 = log2_of(hc);
+  p.hash_limit = hc - hc / 4;
+  const uint32_t st_cap = pow2_at_least((uint32_t)(kStepTableFactor * width) * p.cand_cap);
+  p.step_cap = st_cap;
+  p.step_log2 = log2_of(st_cap);
+  p.words_per_team = p.q_words + 4 * p.pool_cap + p.hash_cap + 2 * st_cap +
+                     5 * (uint32_t)width * p.cand_cap + 32 + 64;
+  p.words_per_team = round_up(p.words_per_team, 4);
+  return p;
+}
+
+int warp_search_occupancy(const GraphView &g, const SmemPlan &p, int warps_per_block) {
+  WarpFn fn = warp_fn(g);
+  const size_t smem = (size_t)p.words_per_team * 4 * warps_per_block;
+  if (cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return 0;
+  int blocks = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, (const void *)fn, warps_per_block * 32,
+                                                    smem) != cudaSuccess)
+    return 0;
+  return blocks;
+}
+
+cudaError_t launch_warp_search(const GraphView &g, const BatchArgs &a, const SmemPlan &p,
+                               int warps_per_block, int blocks, cudaStream_t stream) {
+  WarpFn fn = warp_fn(g);
+  const size_t smem = (size_t)p.words_per_team * 4 * warps_per_block;
+  cudaError_t e = cudaFuncSetAttribute((const void *)fn,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  if (blocks <= 0) blocks = (int)((a.nq + warps_per_block - 1) / warps_per_block);
+  if (blocks <= 0) return cudaSuccess;
+  fn<<<blocks, warps_per_block * 32, smem, stream>>>(g, a, p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_intra_search(const GraphView &g, const BatchArgs &a, const SmemPlan &p,
+                                int width, cudaStream_t stream) {
+  IntraFn fn = intra_fn(g);
+  const size_t smem = (size_t)p.words_per_team * 4;
+  cudaError_t e = cudaFuncSetAttribute((const void *)fn,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  if (a.nq == 0) return cudaSuccess;
+  fn<<<a.nq, width * 32, smem, stream>>>(g, a, p, width);
+  return cudaGetLastError();
+}
+
+}  // namespace ssb

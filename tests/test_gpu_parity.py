@@ -1,0 +1,283 @@
+"""Parity of the CUDA search path with the oracle and the reference.
+
+Every search here goes through libscattersearch_b200.so's C ABI.  The bar is
+bit-exact: identical id lists and identical float32 distance bits against the
+oracle (the project's C restatement, itself pinned to the reference by
+test_oracle.py), and identical ids against the reference's own golden outputs
+for every query whose initial pool has no exactly tied distances.
+"""
+import os
+import threading
+
+import numpy as np
+import pytest
+
+from conftest import NONE_ID, SEARCH_FIXTURES, fixture_cases, load_fixture
+
+pytestmark = pytest.mark.gpu
+
+
+def _index(base, adj, ep, metric):
+    from scattersearch_b200 import ANNSearch
+    idx = ANNSearch(base.shape[1], base.shape[0], base, metric)
+    idx.SetGraph(adj, int(ep))
+    return idx
+
+
+def _same_bits(a, b):
+    return np.array_equal(np.asarray(a, np.float32).view(np.uint32),
+                          np.asarray(b, np.float32).view(np.uint32))
+
+
+@pytest.mark.parametrize("name", SEARCH_FIXTURES)
+def test_plain_search_matches_reference_and_oracle(oracle_lib, name):
+    O = oracle_lib
+    fx = load_fixture(name)
+    idx = _index(fx["base"], fx["adj"], fx["ep"], int(fx["metric"]))
+    for K, L in fixture_cases(fx):
+        o_ids, o_d, _, _ = O.search(fx["base"], fx["adj"], int(fx["ep"]), int(fx["metric"]),
+                                    fx["queries"], K, L)
+        ref = fx[f"ids_K{K}_L{L}"]
+        tie = fx[f"init_tie_L{L}"]
+        for i, q in enumerate(fx["queries"]):
+            ids, d = idx.search(q, K, L)
+            assert np.array_equal(ids, o_ids[i]), (name, K, L, i)
+            assert _same_bits(d, o_d[i]), (name, K, L, i)
+            if not tie[i]:
+                assert np.array_equal(ids, ref[i]), (name, K, L, i)
+    idx.close()
+
+
+@pytest.mark.parametrize("name", SEARCH_FIXTURES)
+def test_batched_equals_plain(oracle_lib, name):
+    O = oracle_lib
+    fx = load_fixture(name)
+    idx = _index(fx["base"], fx["adj"], fx["ep"], int(fx["metric"]))
+    for K, L in fixture_cases(fx):
+        ids, d = idx.search_batch(fx["queries"], K, L)
+        o_ids, o_d, _, _ = O.search(fx["base"], fx["adj"], int(fx["ep"]), int(fx["metric"]),
+                                    fx["queries"], K, L)
+        assert np.array_equal(ids, o_ids)
+        assert _same_bits(d, o_d)
+        for wpb in (1, 2, 8):
+            idx.set_tuning(warps_per_block=wpb)
+            ids2, d2 = idx.search_batch(fx["queries"], K, L)
+            assert np.array_equal(ids2, ids) and _same_bits(d2, d)
+        idx.set_tuning()
+    idx.close()
+
+
+def test_uneven_batch_equals_per_query(oracle_lib):
+    O = oracle_lib
+    fx = load_fixture("search_l2_d200")
+    idx = _index(fx["base"], fx["adj"], fx["ep"], 0)
+    rng = np.random.default_rng(11)
+    nq = len(fx["queries"])
+    Ks = rng.choice(np.array([1, 10, 100], np.int32), nq)
+    Ls = np.maximum(Ks, rng.integers(32, 513, nq)).astype(np.int32)
+    ids, d = idx.search_batch_uneven(fx["queries"], Ks, Ls)
+    o_ids, o_d, _, _ = O.search(fx["base"], fx["adj"], int(fx["ep"]), 0, fx["queries"], Ks=Ks,
+                                Ls=Ls)
+    assert np.array_equal(ids, o_ids) and _same_bits(d, o_d)
+    off = 0
+    for i in range(nq):
+        one, od = idx.search(fx["queries"][i], int(Ks[i]), int(Ls[i]))
+        assert np.array_equal(one, ids[off:off + Ks[i]])
+        off += Ks[i]
+    idx.close()
+
+
+@pytest.mark.parametrize("W", [1, 2, 4, 8])
+def test_intra_query_matches_restatement(oracle_lib, W):
+    O = oracle_lib
+    fx = load_fixture("search_l2_d200")
+    idx = _index(fx["base"], fx["adj"], fx["ep"], 0)
+    o_ids, o_d, _, _ = O.search(fx["base"], fx["adj"], int(fx["ep"]), 0, fx["queries"], 10, 100,
+                                W=W)
+    ids, d = idx.search_intra_batch(fx["queries"], 10, 100, W)
+    assert np.array_equal(ids, o_ids)
+    assert _same_bits(d, o_d)
+    one, _ = idx.search_intra(fx["queries"][0], 10, 100, W)
+    assert np.array_equal(one, o_ids[0])
+    if W == 1:
+        plain, _ = idx.search_batch(fx["queries"], 10, 100)
+        assert np.array_equal(ids, plain)
+    idx.close()
+
+
+def _synthetic(seed, n, dim, R, metric, clusters=8):
+    from scattersearch_b200 import graph
+    rng = np.random.default_rng(seed)
+    means = rng.standard_normal((clusters, dim)).astype(np.float32)
+    X = (means[rng.integers(0, clusters, n)] + 0.4 * rng.standard_normal((n, dim))).astype(
+        np.float32)
+    Q = (means[rng.integers(0, clusters, 128)] + 0.4 * rng.standard_normal((128, dim))).astype(
+        np.float32)
+    if metric == 1:
+        X /= np.linalg.norm(X, axis=1, keepdims=True)
+        Q /= np.linalg.norm(Q, axis=1, keepdims=True)
+    adj, ep = graph.build_graph(X, R=R, knn_k=2 * R, device="cpu")
+    return X, Q, adj, ep
+
+
+@pytest.mark.parametrize("dim,R,metric", [(128, 64, 0), (96, 32, 1), (13, 16, 0), (200, 32, 1),
+                                          (256, 100, 0)])
+def test_synthetic_shapes(oracle_lib, dim, R, metric):
+    """Generic dims (13 is not a multiple of 8, 256 has no specialisation)
+    and wide graphs (R = 64 and 100 take two and four 32-id chunks)."""
+    O = oracle_lib
+    X, Q, adj, ep = _synthetic(dim + R, 4000, dim, R, metric)
+    idx = _index(X, adj, ep, metric)
+    for K, L in ((10, 10), (10, 64), (32, 200)):
+        ids, d = idx.search_batch(Q, K, L)
+        o_ids, o_d, _, _ = O.search(X, adj, ep, metric, Q, K, L)
+        assert np.array_equal(ids, o_ids), (dim, R, K, L)
+        assert _same_bits(d, o_d)
+    idx.close()
+
+
+def test_visited_spill_to_global_bitset(oracle_lib):
+    """A visited hash far smaller than the query's visited set forces the
+    overflow into the global bitset; results must not change."""
+    O = oracle_lib
+    X, Q, adj, ep = _synthetic(5, 20000, 64, 32, 0, clusters=4)
+    idx = _index(X, adj, ep, 0)
+    o_ids, o_d, ndc, _ = O.search(X, adj, ep, 0, Q, 50, 400)
+    assert ndc.max() > 768  # the smallest hash (1024 slots, 768 before spilling) overflows
+    idx.set_tuning(warps_per_block=4, hash_cap=1024)
+    for _ in range(2):  # second pass checks the bitsets were cleared
+        ids, d = idx.search_batch(Q, 50, 400)
+        assert np.array_equal(ids, o_ids) and _same_bits(d, o_d)
+    for W in (1, 4):
+        o_w, _, _, _ = O.search(X, adj, ep, 0, Q[:16], 50, 400, W=W)
+        ids, _ = idx.search_intra_batch(Q[:16], 50, 400, W)
+        assert np.array_equal(ids, o_w)
+    idx.close()
+
+
+def test_edge_cases(oracle_lib):
+    O = oracle_lib
+    rng = np.random.default_rng(9)
+    X = rng.standard_normal((50, 16)).astype(np.float32)
+    adj = np.full((50, 8), NONE_ID, dtype=np.uint32)
+    for i in range(50):
+        adj[i, :6] = rng.choice(50, 6, replace=False)
+    adj[7, :4] = [7, 9, 9, 3]         # self loop and repeated id in the entry row
+    adj[20, :] = NONE_ID              # a node without neighbours
+    idx = _index(X, adj, 7, 0)
+    for K, L in ((1, 1), (4, 4), (8, 50), (50, 50)):
+        ids, d = idx.search_batch(X[:10], K, L)
+        o_ids, o_d, _, _ = O.search(X, adj, 7, 0, X[:10], K, L)
+        assert np.array_equal(ids, o_ids) and _same_bits(d, o_d), (K, L)
+    # entry point without neighbours: nothing expands, slots hold id 0 / 0.0
+    idx.SetGraph(adj, 20)
+    ids, d = idx.search(X[0], 5, 10)
+    assert (ids == 0).all() and (d == 0).all()
+    from scattersearch_b200 import SearchError
+    with pytest.raises(SearchError):
+        idx.search(X[0], 11, 10)       # K > L
+    with pytest.raises(SearchError):
+        idx.search(X[0], 1, 5000)      # L > SS_MAX_L
+    with pytest.raises(SearchError):
+        idx.search_intra(X[0], 1, 10, 17)
+    idx.close()
+
+
+def test_graph_validation_and_loader(tmp_path):
+    from scattersearch_b200 import ANNSearch, SearchError, io
+    X = np.random.default_rng(1).standard_normal((40, 8)).astype(np.float32)
+    idx = ANNSearch(8, 40, X, 0)
+    with pytest.raises(SearchError):
+        idx.search(X[0], 1, 4)         # no graph yet
+    with pytest.raises(SearchError):
+        idx.LoadGraph(str(tmp_path / "missing.nsg"))
+    g = load_fixture("nsg_golden")
+    p = tmp_path / "g.nsg"
+    g["raw"].tofile(p)
+    idx.LoadGraph(str(p))
+    assert idx.default_ep == int(g["ep"])
+    got = idx.graph_table(g["adj"].shape[1])
+    assert np.array_equal(got, g["adj"])
+    # truncated file
+    g["raw"][:-3].tofile(tmp_path / "t.nsg")
+    with pytest.raises(SearchError):
+        idx.LoadGraph(str(tmp_path / "t.nsg"))
+    # id out of range
+    bad = g["adj"].copy()
+    bad[0, 0] = 40
+    io.write_nsg(str(tmp_path / "b.nsg"), bad, 0)
+    with pytest.raises(SearchError):
+        idx.LoadGraph(str(tmp_path / "b.nsg"))
+    with pytest.raises(SearchError):
+        idx.SetGraph(bad, 0)
+    idx.close()
+
+
+def test_device_api_matches_host_api(oracle_lib):
+    import torch
+    fx = load_fixture("search_ip_d96")
+    idx = _index(fx["base"], fx["adj"], fx["ep"], 1)
+    ids_h, d_h = idx.search_batch(fx["queries"], 20, 64)
+    q = torch.as_tensor(fx["queries"]).cuda()
+    nq = q.shape[0]
+    ids = torch.empty((nq, 20), dtype=torch.int32, device="cuda")
+    d = torch.empty((nq, 20), dtype=torch.float32, device="cuda")
+    ndc = torch.empty(nq, dtype=torch.int32, device="cuda")
+    hops = torch.empty(nq, dtype=torch.int32, device="cuda")
+    s = torch.cuda.current_stream()
+    idx.search_batch_device(q, nq, ids, d, K=20, L=64, ndc=ndc, hops=hops, stream=s.cuda_stream)
+    s.synchronize()
+    assert idx.batch_status() == 0
+    assert np.array_equal(ids.cpu().numpy().view(np.uint32), ids_h)
+    assert _same_bits(d.cpu().numpy(), d_h)
+    _, _, o_ndc, o_hops = oracle_lib.search(fx["base"], fx["adj"], int(fx["ep"]), 1, fx["queries"],
+                                            20, 64)
+    assert np.array_equal(ndc.cpu().numpy().view(np.uint32), o_ndc)
+    assert np.array_equal(hops.cpu().numpy().view(np.uint32), o_hops)
+    idx.close()
+
+
+def test_concurrent_callers_share_one_index(oracle_lib):
+    fx = load_fixture("search_l2_d64")
+    idx = _index(fx["base"], fx["adj"], fx["ep"], 0)
+    o_ids, _, _, _ = oracle_lib.search(fx["base"], fx["adj"], int(fx["ep"]), 0, fx["queries"], 10,
+                                       50)
+    errors = []
+
+    def worker(t):
+        try:
+            for i in range(t, len(fx["queries"]), 4):
+                ids, _ = idx.search(fx["queries"][i], 10, 50)
+                if not np.array_equal(ids, o_ids[i]):
+                    errors.append(i)
+        except Exception as e:  # pragma: no cover - reported below
+            errors.append(repr(e))
+
+    th = [threading.Thread(target=worker, args=(t,)) for t in range(4)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert not errors
+    idx.close()
+
+
+def test_reference_style_driver_surface(oracle_lib):
+    """The reference drivers' calling pattern: SearchArraySimulation with a
+    caller-owned flags object and a preallocated indices vector."""
+    fx = load_fixture("search_l2_d64")
+    idx = _index(fx["base"], fx["adj"], fx["ep"], 0)
+
+    class Flags:
+        resets = 0
+
+        def reset(self):
+            Flags.resets += 1
+
+    flags = Flags()
+    tmp = [0] * 10
+    out = idx.SearchArraySimulation(fx["queries"][0], 0, 10, 50, flags, tmp)
+    assert tmp == out.tolist() and Flags.resets == 1
+    out2 = idx.MultiThreadSearchArraySimulationWithET(fx["queries"][0], 0, 10, 50, 1, flags, tmp)
+    assert np.array_equal(out, out2)
+    idx.close()
