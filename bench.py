@@ -179,6 +179,8 @@ def build_workload(args, rank, world, device):
     Q = torch.from_numpy(queries).to(device)
     gt, _ = graph.bruteforce(X, Q, 10, w.metric)
     log(f"ground truth in {time.time() - t0:.1f}s")
+    if device != "cpu" and torch.cuda.is_available():
+        torch.cuda.empty_cache()  # hand the graph build's scratch back to the driver
     return dict(spec=spec, w=w, X=X, queries=queries, Q=Q, adj=adj, ep=ep,
                 gt=gt.cpu().numpy(), metric=w.metric, K=spec["K"])
 
@@ -210,13 +212,15 @@ def time_reference(wl, L, seconds, fast=True, warm=1):
     ref.search(q[:probe], K, L, nthreads=th)
     rate = probe / max(1e-6, time.perf_counter() - t0)
     sample = int(min(len(q), max(probe, rate * seconds)))
+    reps = max(1, int(round(rate * seconds / sample)))
     for _ in range(warm):
         ref.search(q[:min(sample, probe)], K, L, nthreads=th)
     t0 = time.perf_counter()
-    ids = ref.search(q[:sample], K, L, nthreads=th)
+    for _ in range(reps):
+        ids = ref.search(q[:sample], K, L, nthreads=th)
     dt = time.perf_counter() - t0
     ref.close()
-    return sample / dt, sample, ids, th
+    return sample * reps / dt, (sample, reps), ids, th
 
 
 def run_reference_arm(args):
@@ -240,20 +244,25 @@ def run_reference_arm(args):
     t0 = time.perf_counter()
     ref.search(q[:probe], K, L, nthreads=th)
     rate = probe / max(1e-6, time.perf_counter() - t0)
-    per_step = int(min(len(q), max(probe, rate * args.cpu_seconds / 2)))
+    # a step is a bounded sample of the workload: about cpu_seconds/steps of
+    # host work, the whole batch repeated when it is shorter than that
+    per_step = int(min(len(q), max(probe, rate * args.cpu_seconds / max(1, args.steps))))
+    reps = max(1, int(round(rate * args.cpu_seconds / max(1, args.steps) / per_step)))
     for _ in range(args.warmup):
-        ref.search(q[:per_step], K, L, nthreads=th)
+        ref.search(q[:min(per_step, probe)], K, L, nthreads=th)
     times = []
     ids = None
     for s in range(args.steps):
         t0 = time.perf_counter()
-        ids = ref.search(q[:per_step], K, L, nthreads=th)
+        for _ in range(reps):
+            ids = ref.search(q[:per_step], K, L, nthreads=th)
         times.append(time.perf_counter() - t0)
     ref.close()
     total = sum(times)
-    qps = per_step * args.steps / total
+    qps = per_step * reps * args.steps / total
     rec = recall_at_10(ids, wl["gt"][:per_step])
-    sample = f"first {per_step} of {len(q)} queries per step, K={K}, L={L}"
+    sample = (f"first {per_step} of {len(q)} queries x{reps} per step, K={K}, L={L}, "
+              f"-Ofast build, OpenMP over queries, one visited bitset per thread")
     out = {
         "impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -437,11 +446,12 @@ def run_ours(args):
         from oracle import oracle as O
         kind = "reference" if O.have_reference(fast=True) else None
         if kind:
-            cqps, sample, cids, th = time_reference(wl, L, args.cpu_seconds)
+            cqps, (sample, reps), cids, th = time_reference(wl, L, args.cpu_seconds)
             out["cpu_baseline"] = {
                 "value": cqps, "unit": "queries/s", "cores": th, "kind": kind,
-                "sample": f"first {sample} of {nq} queries, K={K}, L={L}, reference "
-                          "SearchArraySimulation built -Ofast, OpenMP over queries",
+                "sample": f"first {sample} of {nq} queries x{reps} passes, K={K}, L={L}, "
+                          "reference SearchArraySimulation built -Ofast, OpenMP over queries, "
+                          "one visited bitset per thread",
                 "ids_equal_gpu_fraction": float((cids == ids_np[:sample]).all(1).mean())}
         else:
             out["cpu_baseline"] = None

@@ -256,6 +256,6 @@ class ANNSearch:
         self._check(self._lib.ss_batch_status(self._h, ctypes.byref(n)))
         return n.value
 
-    def set_tuning(self, warps_per_block: int = 4, hash_cap: int = 0, blocks_per_sm_cap: int = 0):
+    def set_tuning(self, warps_per_block: int = 0, hash_cap: int = 0, blocks_per_sm_cap: int = 0):
         self._check(self._lib.ss_set_tuning(self._h, int(warps_per_block), int(hash_cap),
                                             int(blocks_per_sm_cap)))

@@ -101,8 +101,8 @@ struct ss_index {
   SearchCtx dev_ctx;
   uint32_t dev_last_nq = 0;
 
-  // launch tuning (set by the autotuner through ss_set_tuning)
-  int warps_per_block = 4;
+  // launch tuning (set by the autotuner through ss_set_tuning); 0 = automatic
+  int warps_per_block = 0;
   int hash_cap_override = 0;
   int blocks_per_sm_cap = 0;
 
@@ -230,11 +230,25 @@ int persistent_blocks(ss_index *h, const ssb::SmemPlan &p, int wpb, uint32_t nq)
   return (int)std::max(1L, std::min(full, need));
 }
 
+// Query teams per CTA: the tuned value when set, else the candidate (1, 2,
+// 4, 8) that keeps the most teams resident per SM (ties: larger CTAs).
 int choose_wpb(ss_index *h, const ssb::SmemPlan &p) {
-  int wpb = h->warps_per_block;
-  // shared memory per CTA must fit the 227 KB opt-in limit
-  while (wpb > 1 && (size_t)p.words_per_team * 4 * wpb > 227 * 1024) wpb >>= 1;
-  return wpb;
+  auto fits = [&](int w) { return (size_t)p.words_per_team * 4 * w <= 227 * 1024; };
+  if (h->warps_per_block > 0) {
+    int wpb = h->warps_per_block;
+    while (wpb > 1 && !fits(wpb)) wpb >>= 1;
+    return wpb;
+  }
+  int best = 1, best_teams = -1;
+  for (int w = 1; w <= 8; w <<= 1) {
+    if (!fits(w)) break;
+    const int teams = ssb::warp_search_occupancy(h->view(), p, w) * w;
+    if (teams >= best_teams) {
+      best_teams = teams;
+      best = w;
+    }
+  }
+  return best;
 }
 
 // Core batched launch into caller-provided device buffers on `stream`.
@@ -708,8 +722,9 @@ int ss_search_intra_batch_device(ss_index *h, const float *queries, uint32_t nq,
 
 int ss_set_tuning(ss_index *h, int warps_per_block, int hash_cap, int blocks_per_sm_cap) {
   if (!h) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null index handle");
-  if (warps_per_block < 1 || warps_per_block > 8 || (warps_per_block & (warps_per_block - 1)))
-    return set_err(h, SS_ERR_INVALID_ARGUMENT, "warps_per_block must be 1, 2, 4 or 8");
+  if (warps_per_block < 0 || warps_per_block > 8 ||
+      (warps_per_block & (warps_per_block - 1)))
+    return set_err(h, SS_ERR_INVALID_ARGUMENT, "warps_per_block must be 0 (auto), 1, 2, 4 or 8");
   h->warps_per_block = warps_per_block;
   h->hash_cap_override = hash_cap > 0 ? hash_cap : 0;
   h->blocks_per_sm_cap = blocks_per_sm_cap > 0 ? blocks_per_sm_cap : 0;

@@ -42,9 +42,10 @@ struct SmemPlan {
   uint32_t q_words;     // nb*8
   uint32_t pool_cap;    // >= max L of the launch, multiple of 32
   uint32_t cand_cap;    // candidates per step (multiple of 32)
-  uint32_t hash_cap;    // power of two
-  uint32_t hash_log2;
+  uint32_t hash_cap;    // slots, power of two
+  uint32_t hash_log2;   // intra kernel: log2(slots); warp kernel: log2(buckets of 8)
   uint32_t hash_limit;  // entries before spilling to the global bitset
+  uint32_t qh_rbits;    // warp kernel: tag remainder bits of the visited hash
   uint32_t step_cap;    // CTA kernel: step-local dedupe table (power of two)
   uint32_t step_log2;
   uint32_t words_per_team;

@@ -20,6 +20,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+#include <set>
+#include <utility>
+
 #include "ss_internal.h"
 
 namespace ssb {
@@ -267,11 +271,162 @@ __device__ __forceinline__ bool visited_test(const Visited &v, uint32_t id) {
 }
 
 // ------------------------------------------------------- warp per query ---
+// Visited set of the warp kernel: an exact two-choice bucketed hash in
+// shared memory.  Bucket = 8 slots of 16 bits (one 16-byte row, read with a
+// single LDS.128).  An id is mixed by two multiplications with odd constants
+// modulo 2^B (2^B >= n); each product is a bijection of [0, 2^B), so its high
+// bits (the bucket) plus its low bits (the 16-bit tag) identify the id
+// exactly.  Tags of the second choice carry bit 15, so a tag names both the
+// id and the choice; 0xFFFF marks an empty slot.  When both buckets of an id
+// are full the id goes to the per-team global bitset instead, and from then
+// on every lookup that misses the table also consults the bitset.
+struct QHash {
+  uint4 *bkt;
+  uint32_t bbits, rbits, rmask, bmask;
+  uint32_t *bits;  // global spill bitset (n bits), may be null
+  bool spilled;
+};
+
+constexpr uint32_t kMix1 = 0x9E3779B1u;
+constexpr uint32_t kMix2 = 0x7FEB352Du;
+constexpr uint32_t kEmptyTag = 0xFFFFu;
+
+__device__ __forceinline__ void qh_keys(const QHash &h, uint32_t id, uint32_t &b1, uint32_t &t1,
+                                        uint32_t &b2, uint32_t &t2) {
+  const uint32_t f1 = (id * kMix1) & h.bmask;
+  const uint32_t f2 = (id * kMix2) & h.bmask;
+  b1 = f1 >> h.rbits;
+  t1 = f1 & h.rmask;
+  b2 = f2 >> h.rbits;
+  t2 = (f2 & h.rmask) | 0x8000u;
+}
+
+__device__ __forceinline__ bool bucket_has(uint4 v, uint32_t t) {
+  const uint32_t tt = t | (t << 16);
+  return (__vcmpeq2(v.x, tt) | __vcmpeq2(v.y, tt) | __vcmpeq2(v.z, tt) | __vcmpeq2(v.w, tt)) != 0u;
+}
+
+// 8-bit mask of empty slots (slot s = 16-bit half s of the bucket).
+__device__ __forceinline__ uint32_t bucket_empty(uint4 v) {
+  const uint32_t e0 = __vcmpeq2(v.x, 0xFFFFFFFFu), e1 = __vcmpeq2(v.y, 0xFFFFFFFFu);
+  const uint32_t e2 = __vcmpeq2(v.z, 0xFFFFFFFFu), e3 = __vcmpeq2(v.w, 0xFFFFFFFFu);
+  return (e0 & 1u) | ((e0 >> 15) & 2u) | ((e1 & 1u) << 2) | ((e1 >> 13) & 8u) |
+         ((e2 & 1u) << 4) | ((e2 >> 11) & 32u) | ((e3 & 1u) << 6) | ((e3 >> 9) & 128u);
+}
+
+// 16-byte shared-memory load that is never cached in registers or reordered
+// across other shared-memory accesses (buckets change under concurrent CAS).
+__device__ __forceinline__ uint4 lds128(const uint4 *p) {
+  uint4 v;
+  const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+  asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "r"(a)
+               : "memory");
+  return v;
+}
+
+// Marks `id` visited.  Returns true when it was not visited before.  The
+// calling lanes of one warp must hold distinct ids.  Sets `full` when the id
+// fit in neither bucket (it was then NOT recorded).
+__device__ __forceinline__ bool qh_insert(const QHash &h, uint32_t id, bool &full) {
+  uint32_t b1, t1, b2, t2;
+  qh_keys(h, id, b1, t1, b2, t2);
+  unsigned short *slots = reinterpret_cast<unsigned short *>(h.bkt);
+  full = false;
+  for (int attempt = 0; attempt < 17; ++attempt) {
+    const uint4 v1 = lds128(h.bkt + b1);
+    const uint4 v2 = lds128(h.bkt + b2);
+    if (bucket_has(v1, t1) || bucket_has(v2, t2)) return false;
+    const uint32_t e1 = bucket_empty(v1), e2 = bucket_empty(v2);
+    if ((e1 | e2) == 0u) {
+      full = true;
+      return false;
+    }
+    const bool use1 = __popc(e1) >= __popc(e2);
+    const uint32_t b = use1 ? b1 : b2, t = use1 ? t1 : t2, e = use1 ? e1 : e2;
+    const uint32_t s = __ffs(e) - 1;
+    if (atomicCAS(slots + b * 8 + s, (unsigned short)kEmptyTag, (unsigned short)t) == kEmptyTag)
+      return true;
+  }
+  full = true;  // unreachable: each failed CAS means a slot was taken
+  return false;
+}
+
+__device__ __forceinline__ bool qh_contains(const QHash &h, uint32_t id) {
+  uint32_t b1, t1, b2, t2;
+  qh_keys(h, id, b1, t1, b2, t2);
+  const uint4 v1 = lds128(h.bkt + b1);
+  const uint4 v2 = lds128(h.bkt + b2);
+  return bucket_has(v1, t1) || bucket_has(v2, t2);
+}
+
+// Warp-wide visit of one id per lane (`valid` lanes hold distinct ids).
+// Returns true for ids that were not visited before.  All 32 lanes call it.
+__device__ __forceinline__ bool qh_visit_warp(QHash &h, uint32_t id, bool valid) {
+  bool fresh = false;
+  if (!h.spilled) {
+    bool full = false;
+    if (valid) fresh = qh_insert(h, id, full);
+    const unsigned fm = __ballot_sync(kFull, full);
+    if (fm) {
+      h.spilled = true;
+      if (full && h.bits) {  // not in the table: record it in the bitset (never set before)
+        const uint32_t bit = 1u << (id & 31u);
+        fresh = (atomicOr(h.bits + (id >> 5), bit) & bit) == 0u;
+      }
+    }
+  } else if (valid && h.bits) {
+    if (!qh_contains(h, id)) {
+      const uint32_t bit = 1u << (id & 31u);
+      fresh = (atomicOr(h.bits + (id >> 5), bit) & bit) == 0u;
+    }
+  }
+  return fresh;
+}
+
+// Starts an L2 prefetch of the base rows of cid[0..nc) (one bulk prefetch
+// per row, no registers held), so every 16-candidate pass of
+// eval_candidates after the first finds its rows in L2 and the first
+// overlaps all of them.
+__device__ __forceinline__ void prefetch_rows(const GraphView &g, const uint32_t *cid, int nc,
+                                              int lane) {
+  const uint32_t bytes = g.nb * 32u;
+  for (int e = lane; e < nc; e += 32) {
+    const float *row = g.base + (size_t)cid[e] * (size_t)(g.nb * 8);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(row), "r"(bytes) : "memory");
+  }
+}
+
+// Keys of cid[0..nc) into ckey[0..nc): prefetch every row, then 16 per pass.
+template <int NB>
+__device__ __forceinline__ void eval_all(const GraphView &g, const float *qs, const uint32_t *cid,
+                                         uint32_t *ckey, int nc, int lane) {
+  if (nc > 16) prefetch_rows(g, cid, nc, lane);
+  eval_candidates<NB>(g, qs, cid, ckey, nc, lane);
+}
+
+// Branch-free binary searches over ascending arrays (warp-uniform trip
+// counts, so lanes never diverge).  `top` = largest power of two <= n.
+__device__ __forceinline__ int count_le_bf(const uint32_t *a, int n, int top, uint32_t key) {
+  int pos = 0;
+  for (int step = top; step > 0; step >>= 1) {
+    const int np = pos + step;
+    const uint32_t v = a[min(np, n) - 1];
+    pos = (np <= n && v <= key) ? np : pos;
+  }
+  return pos;
+}
+
+__device__ __forceinline__ int floor_pow2(int n) { return n > 0 ? 1 << (31 - __clz(n)) : 0; }
+
 struct WarpSmem {
   float *q;
-  uint32_t *pk, *pid;          // pool keys / ids (bit 31 of id = explored)
-  uint32_t *cand_id, *cand_key, *sk;
-  uint32_t *hash;
+  uint32_t *pk, *pid;              // pool keys / ids (bit 31 of id = explored)
+  uint32_t *cid, *ckey;            // this hop's fresh candidates, adjacency order
+  uint32_t *ak, *aid;              // accepted candidates, adjacency order
+  uint32_t *sk, *sid;              // accepted candidates, sorted
+  uint4 *bkt;                      // visited hash buckets
 };
 
 __device__ __forceinline__ WarpSmem carve_warp(uint32_t *base, const SmemPlan &p) {
@@ -282,18 +437,66 @@ __device__ __forceinline__ WarpSmem carve_warp(uint32_t *base, const SmemPlan &p
   base += p.pool_cap;
   s.pid = base;
   base += p.pool_cap;
-  s.cand_id = base;
+  s.cid = base;
   base += p.cand_cap;
-  s.cand_key = base;
+  s.ckey = base;
+  base += p.cand_cap;
+  s.ak = base;
+  base += p.cand_cap;
+  s.aid = base;
   base += p.cand_cap;
   s.sk = base;
   base += p.cand_cap;
-  s.hash = base;
+  s.sid = base;
+  base += p.cand_cap;
+  s.bkt = reinterpret_cast<uint4 *>(base);
   return s;
 }
 
-// One query, one warp.  Steps per hop (batch-merge form of
-// annsearch.cpp:218-253):
+// Sorts the n candidates (keys ks[0..n), ids is[0..n), adjacency order) by
+// (key, position) into sk/sid: lane i ranks its candidate by counting the
+// candidates that precede it.  n <= 32*ITEMS.
+template <int ITEMS>
+__device__ __forceinline__ void rank_sort(const uint32_t *ks, const uint32_t *is, int n,
+                                          uint32_t *sk, uint32_t *sid, int lane) {
+  uint32_t mk[ITEMS];
+  int rank[ITEMS];
+#pragma unroll
+  for (int t = 0; t < ITEMS; ++t) {
+    mk[t] = (t * 32 + lane) < n ? ks[t * 32 + lane] : 0u;
+    rank[t] = 0;
+  }
+  for (int j = 0; j < n; ++j) {
+    const uint32_t kj = ks[j];
+#pragma unroll
+    for (int t = 0; t < ITEMS; ++t) {
+      const int i = t * 32 + lane;
+      rank[t] += (kj < mk[t]) || (kj == mk[t] && j < i);
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < ITEMS; ++t) {
+    const int i = t * 32 + lane;
+    if (i < n) {
+      sk[rank[t]] = mk[t];
+      sid[rank[t]] = is[i];
+    }
+  }
+}
+
+// Loads this lane's share of a node's adjacency row.
+template <int RCH>
+__device__ __forceinline__ void load_row(const GraphView &g, uint32_t node, int lane,
+                                         uint32_t (&row)[RCH]) {
+  const uint32_t *nrow = g.adj + (size_t)node * g.rstride;
+#pragma unroll
+  for (int c = 0; c < RCH; ++c) {
+    const int m = c * 32 + lane;
+    row[c] = m < (int)g.rstride ? __ldg(nrow + m) : kNoneId;
+  }
+}
+
+// One query, one warp.  Each hop (batch-merge form of annsearch.cpp:218-253):
 //   1. expand the first unexplored pool slot (all slots before `cursor` are
 //      explored);
 //   2. read its adjacency row; drop ids already visited and mark the rest
@@ -303,6 +506,7 @@ __device__ __forceinline__ WarpSmem carve_warp(uint32_t *base, const SmemPlan &p
 //   5. sort accepted candidates by (d, adjacency position) and stable-merge
 //      them into the pool, older entries first on ties, truncated to L
 //      (InsertIntoPool upper-bound insert, util.h:56-75; :242-243).
+// The adjacency row of the hop after this one is loaded while the merge runs.
 template <int NB, int RCH>
 __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qsrc, int K, int L,
                                 uint32_t *out_ids, float *out_dists, uint32_t *out_ndc,
@@ -312,15 +516,16 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
   const unsigned lanemask_lt = (1u << lane) - 1u;
   const int qw = (int)g.nb * 8;
   for (int i = lane; i < qw; i += 32) s.q[i] = i < (int)g.dim ? qsrc[i] : 0.f;
-  for (uint32_t i = lane; i < p.hash_cap; i += 32) s.hash[i] = kNoneId;
+  const uint32_t nbk = 1u << p.hash_log2;
+  for (uint32_t i = lane; i < nbk; i += 32) s.bkt[i] = make_uint4(~0u, ~0u, ~0u, ~0u);
   __syncwarp();
 
-  Visited vis;
-  vis.tab = s.hash;
-  vis.mask = p.hash_cap - 1;
-  vis.log2cap = p.hash_log2;
-  vis.limit = p.hash_limit;
-  vis.count = 0;
+  QHash vis;
+  vis.bkt = s.bkt;
+  vis.bbits = p.hash_log2;
+  vis.rbits = p.qh_rbits;
+  vis.rmask = (1u << p.qh_rbits) - 1u;
+  vis.bmask = (p.hash_log2 + p.qh_rbits >= 32) ? ~0u : ((1u << (p.hash_log2 + p.qh_rbits)) - 1u);
   vis.bits = spill;
   vis.spilled = false;
 
@@ -332,39 +537,31 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
   // ties keep adjacency order.
   int size = 0;
   {
-    const uint32_t *erow = g.adj + (size_t)g.ep * g.rstride;
+    uint32_t row[RCH];
+    load_row<RCH>(g, g.ep, lane, row);
 #pragma unroll
     for (int c = 0; c < RCH; ++c) {
       const int m = c * 32 + lane;
-      const uint32_t id = m < (int)g.rstride ? __ldg(erow + m) : kNoneId;
-      const bool valid = id != kNoneId && m < L;
-      if (valid) {
-        s.cand_id[m] = id;
-        visit(vis, id);
-      }
+      const bool valid = row[c] != kNoneId && m < L;
+      const unsigned peers = __match_any_sync(kFull, row[c]);
+      const bool leader = valid && (peers & lanemask_lt) == 0u;
+      if (valid) s.cid[m] = row[c];
+      qh_visit_warp(vis, row[c], leader);
       size += __popc(__ballot_sync(kFull, valid));
     }
-    vis.count = size;
     __syncwarp();
-    eval_candidates<NB>(g, s.q, s.cand_id, s.cand_key, size, lane);
+    eval_all<NB>(g, s.q, s.cid, s.ckey, size, lane);
     ndc += size;
     __syncwarp();
-    uint64_t x[RCH];
-#pragma unroll
-    for (int i = 0; i < RCH; ++i) {
-      const int e = i * 32 + lane;
-      x[i] = e < size ? (((uint64_t)s.cand_key[e] << 32) | (uint32_t)e) : kInvalidKey;
-    }
-    warp_sort<RCH>(x, lane);
-#pragma unroll
-    for (int i = 0; i < RCH; ++i) {
-      const int e = i * 32 + lane;
-      if (e < size) {
-        s.pk[e] = (uint32_t)(x[i] >> 32);
-        s.pid[e] = s.cand_id[(uint32_t)x[i]];
-      }
-    }
+    rank_sort<RCH>(s.ckey, s.cid, size, s.pk, s.pid, lane);
     __syncwarp();
+  }
+
+  uint32_t pref_node = kNoneId;
+  uint32_t pref_row[RCH];
+  if (size > 0) {
+    pref_node = s.pid[0];
+    load_row<RCH>(g, pref_node, lane, pref_row);
   }
 
   int cursor = 0;
@@ -390,101 +587,153 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
     __syncwarp();
     if (lane == 0) s.pid[k] = node | kExplored;
     ++hops;
-    cursor = k + 1;
+    uint32_t row[RCH];
+    if (node == pref_node) {
+#pragma unroll
+      for (int c = 0; c < RCH; ++c) row[c] = pref_row[c];
+    } else {
+      load_row<RCH>(g, node, lane, row);
+    }
 
-    // 2. adjacency row, in-row dedupe, visited filter, compaction in m order
-    const uint32_t *nrow = g.adj + (size_t)node * g.rstride;
+    // 2. in-row dedupe, visited filter, compaction in m order
     int nc = 0;
 #pragma unroll
     for (int c = 0; c < RCH; ++c) {
-      const int m = c * 32 + lane;
-      const uint32_t id = m < (int)g.rstride ? __ldg(nrow + m) : kNoneId;
-      const bool valid = id != kNoneId;
-      const unsigned peers = __match_any_sync(kFull, id);
+      const bool valid = row[c] != kNoneId;
+      const unsigned peers = __match_any_sync(kFull, row[c]);
       const bool leader = valid && (peers & lanemask_lt) == 0u;
-      if (!vis.spilled && vis.count + 32u > vis.limit) {
-        if (!spill) {
-          status = kStatusVisitedFull;
-          break;
-        }
-        vis.spilled = true;
-      }
-      const bool fresh = leader && visit(vis, id);
+      const bool fresh = qh_visit_warp(vis, row[c], leader);
       const unsigned fm = __ballot_sync(kFull, fresh);
-      if (fresh) s.cand_id[nc + __popc(fm & lanemask_lt)] = id;
+      if (fresh) s.cid[nc + __popc(fm & lanemask_lt)] = row[c];
       nc += __popc(fm);
-      if (!vis.spilled) vis.count += __popc(fm);
     }
-    if (status != kStatusOk) break;
-    if (nc == 0) continue;
+    if (vis.spilled && !spill) {
+      status = kStatusVisitedFull;
+      break;
+    }
+    if (nc == 0) {
+      pref_node = kNoneId;
+      continue;
+    }
     __syncwarp();
 
-    // 3. distances
-    eval_candidates<NB>(g, s.q, s.cand_id, s.cand_key, nc, lane);
+    // 3. distances (rows prefetched to L2 together, then 16 per pass)
+    eval_all<NB>(g, s.q, s.cid, s.ckey, nc, lane);
     ndc += nc;
     __syncwarp();
 
-    // 4. acceptance + sort by (key, m)
-    uint64_t x[RCH];
+    // 4. acceptance (adjacency order), then rank sort by (key, m)
     int na = 0;
 #pragma unroll
-    for (int i = 0; i < RCH; ++i) {
-      const int e = i * 32 + lane;
-      const bool acc = e < nc && s.cand_key[e] < thr;
-      x[i] = acc ? (((uint64_t)s.cand_key[e] << 32) | (uint32_t)e) : kInvalidKey;
-      na += __popc(__ballot_sync(kFull, acc));
+    for (int c = 0; c < RCH; ++c) {
+      const int e = c * 32 + lane;
+      const uint32_t key = e < nc ? s.ckey[e] : 0xFFFFFFFFu;
+      const bool acc = e < nc && key < thr;
+      const unsigned am = __ballot_sync(kFull, acc);
+      if (acc) {
+        const int pos = na + __popc(am & lanemask_lt);
+        s.ak[pos] = key;
+        s.aid[pos] = s.cid[e];
+      }
+      na += __popc(am);
     }
-    if (na == 0) continue;
-    warp_sort<RCH>(x, lane);
+    // next pick if nothing is accepted: first unexplored after k
+    int u = -1;
+    for (int b0 = k + 1; b0 < size; b0 += 32) {
+      const int idx = b0 + lane;
+      const bool un = idx < size && !(s.pid[idx] & kExplored);
+      const unsigned bm = __ballot_sync(kFull, un);
+      if (bm) {
+        u = b0 + __ffs(bm) - 1;
+        break;
+      }
+    }
+    if (na == 0) {
+      pref_node = kNoneId;
+      if (u >= 0) {
+        pref_node = s.pid[u];
+        load_row<RCH>(g, pref_node, lane, pref_row);
+      }
+      cursor = k + 1;
+      continue;
+    }
+    __syncwarp();
+    rank_sort<RCH>(s.ak, s.aid, na, s.sk, s.sid, lane);
+    __syncwarp();
 
     // 5. stable merge into the pool, in place
+    const int top = floor_pow2(size);
     uint32_t nkey[RCH], nid[RCH];
     int npos[RCH];
 #pragma unroll
-    for (int i = 0; i < RCH; ++i) npos[i] = 0;
-#pragma unroll
-    for (int i = 0; i < RCH; ++i) {
-      const int e = i * 32 + lane;
+    for (int c = 0; c < RCH; ++c) {
+      const int e = c * 32 + lane;
+      npos[c] = L;
       if (e < na) {
-        nkey[i] = (uint32_t)(x[i] >> 32);
-        nid[i] = s.cand_id[(uint32_t)x[i]];
-        s.sk[e] = nkey[i];
-        npos[i] = e + count_le(s.pk, size, nkey[i]);
+        nkey[c] = s.sk[e];
+        nid[c] = s.sid[e];
+        npos[c] = e + count_le_bf(s.pk, size, top, nkey[c]);
       }
     }
     const int p0 = __shfl_sync(kFull, npos[0], 0);
-    __syncwarp();
+    // Prefetch the adjacency row of the next expansion: the old pool's
+    // first unexplored slot after k if it precedes the first new entry,
+    // else the first new entry (when it survives truncation).
+    {
+      uint32_t nxt = kNoneId;
+      if (u >= 0 && u < p0) nxt = s.pid[u];
+      else if (p0 < L) nxt = s.sid[0];
+      else if (u >= 0) nxt = s.pid[u];
+      pref_node = nxt;
+      if (nxt != kNoneId) load_row<RCH>(g, nxt, lane, pref_row);
+    }
     // Old entries at and after p0 move up by the number of new keys below
-    // them.  Chunks go from the top down so no entry is overwritten before
-    // it has been read.
-    for (int hi = size; hi > p0; hi -= 32) {
-      const int j = hi - 32 + lane;
-      const bool act = j >= p0;
-      uint32_t ok = 0, oid = 0;
-      int t = 0;
-      if (act) {
-        ok = s.pk[j];
-        oid = s.pid[j];
-        t = j + count_lt(s.sk, na, ok);
+    // them; 128-entry windows from the top down, 4 entries per lane, each
+    // window fully read before it is written.
+    for (int w = ((size - 1) >> 7) << 7; w + 128 > p0 && w >= 0; w -= 128) {
+      const int j0 = w + 4 * lane;
+      const bool any = j0 + 3 >= p0 && j0 < size;
+      uint4 kk = make_uint4(0, 0, 0, 0), ii = make_uint4(0, 0, 0, 0);
+      if (any) {
+        kk = *reinterpret_cast<const uint4 *>(s.pk + j0);
+        ii = *reinterpret_cast<const uint4 *>(s.pid + j0);
+      }
+      int c0 = 0, c1 = 0, c2 = 0, c3 = 0;
+      for (int i = 0; i < na; ++i) {
+        const uint32_t sv = s.sk[i];
+        c0 += kk.x > sv;
+        c1 += kk.y > sv;
+        c2 += kk.z > sv;
+        c3 += kk.w > sv;
       }
       __syncwarp();
-      if (act && t < L) {
-        s.pk[t] = ok;
-        s.pid[t] = oid;
+      if (any) {
+        const uint32_t ks[4] = {kk.x, kk.y, kk.z, kk.w};
+        const uint32_t is[4] = {ii.x, ii.y, ii.z, ii.w};
+        const int cs[4] = {c0, c1, c2, c3};
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const int j = j0 + t;
+          const int dst = j + cs[t];
+          if (j >= p0 && j < size && dst < L) {
+            s.pk[dst] = ks[t];
+            s.pid[dst] = is[t];
+          }
+        }
       }
       __syncwarp();
     }
 #pragma unroll
-    for (int i = 0; i < RCH; ++i) {
-      const int e = i * 32 + lane;
-      if (e < na && npos[i] < L) {
-        s.pk[npos[i]] = nkey[i];
-        s.pid[npos[i]] = nid[i];
+    for (int c = 0; c < RCH; ++c) {
+      const int e = c * 32 + lane;
+      if (e < na && npos[c] < L) {
+        s.pk[npos[c]] = nkey[c];
+        s.pid[npos[c]] = nid[c];
       }
     }
     __syncwarp();
     size = min(L, size + na);
-    cursor = min(cursor, p0);
+    cursor = min(k + 1, p0);
   }
 
   // Results: slots the pool never filled keep the reference's value-
@@ -494,7 +743,7 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
     out_ids[i] = have ? (s.pid[i] & ~kExplored) : 0u;
     if (out_dists) out_dists[i] = have ? key_to_float(s.pk[i]) : 0.f;
   }
-  if (vis.spilled) {
+  if (vis.spilled && spill) {
     for (uint32_t w = lane; w < spill_words; w += 32) spill[w] = 0u;
   }
   if (lane == 0) {
@@ -963,14 +1212,21 @@ SmemPlan plan_warp_smem(const GraphView &g, int L_max, int hash_cap_override) {
   p.q_words = g.nb * 8;
   p.pool_cap = round_up((uint32_t)L_max, 32);
   p.cand_cap = round_up(g.rstride, 32);
-  uint32_t hc = hash_cap_override > 0 ? pow2_at_least((uint32_t)hash_cap_override)
-                                      : pow2_at_least((uint32_t)L_max * 16u);
-  if (hc < 1024) hc = 1024;
-  if (hc > 32768) hc = 32768;
-  p.hash_cap = hc;
-  p.hash_log2 = log2_of(hc);
-  p.hash_limit = hc - hc / 4;  // 75% load, then spill
-  p.words_per_team = p.q_words + 2 * p.pool_cap + 3 * p.cand_cap + p.hash_cap;
+  // visited table: buckets of 8 tags; default about 20 slots per unit of L
+  uint32_t slots = hash_cap_override > 0 ? pow2_at_least((uint32_t)hash_cap_override)
+                                         : pow2_at_least((uint32_t)L_max * 20u);
+  if (slots < 512) slots = 512;
+  if (slots > 65536) slots = 65536;
+  uint32_t bbits = log2_of(slots / 8);
+  uint32_t nbits = 1;
+  while (nbits < 32 && (1ull << nbits) < (unsigned long long)g.n) ++nbits;
+  // tags hold at most 14 remainder bits (bit 15 = second choice, 0xFFFF = empty)
+  if (nbits > bbits + 14) bbits = nbits - 14;
+  p.hash_log2 = bbits;
+  p.qh_rbits = nbits > bbits ? nbits - bbits : 0;
+  p.hash_cap = (1u << bbits) * 8;
+  p.hash_limit = p.hash_cap;
+  p.words_per_team = p.q_words + 2 * p.pool_cap + 6 * p.cand_cap + (1u << bbits) * 4;
   p.words_per_team = round_up(p.words_per_team, 4);
   return p;
 }
@@ -996,12 +1252,32 @@ SmemPlan plan_intra_smem(const GraphView &g, int L_max, int width, int hash_cap_
   return p;
 }
 
+namespace {
+// Raises a kernel's dynamic shared-memory limit to the device's opt-in
+// maximum, once per (device, kernel).  Every launch then only has to fit that
+// maximum, so concurrent callers planning different sizes never lower the
+// limit under one another's launch.
+cudaError_t allow_max_smem(const void *fn) {
+  static std::mutex mu;
+  static std::set<std::pair<int, const void *>> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count({dev, fn})) return cudaSuccess;
+  int optin = 0;
+  e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+  if (e == cudaSuccess) done.insert({dev, fn});
+  return e;
+}
+}  // namespace
+
 int warp_search_occupancy(const GraphView &g, const SmemPlan &p, int warps_per_block) {
   WarpFn fn = warp_fn(g);
   const size_t smem = (size_t)p.words_per_team * 4 * warps_per_block;
-  if (cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem) != cudaSuccess)
-    return 0;
+  if (allow_max_smem((const void *)fn) != cudaSuccess) return 0;
   int blocks = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, (const void *)fn, warps_per_block * 32,
                                                     smem) != cudaSuccess)
@@ -1013,8 +1289,7 @@ cudaError_t launch_warp_search(const GraphView &g, const BatchArgs &a, const Sme
                                int warps_per_block, int blocks, cudaStream_t stream) {
   WarpFn fn = warp_fn(g);
   const size_t smem = (size_t)p.words_per_team * 4 * warps_per_block;
-  cudaError_t e = cudaFuncSetAttribute((const void *)fn,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = allow_max_smem((const void *)fn);
   if (e != cudaSuccess) return e;
   if (blocks <= 0) blocks = (int)((a.nq + warps_per_block - 1) / warps_per_block);
   if (blocks <= 0) return cudaSuccess;
@@ -1026,8 +1301,7 @@ cudaError_t launch_intra_search(const GraphView &g, const BatchArgs &a, const Sm
                                 int width, cudaStream_t stream) {
   IntraFn fn = intra_fn(g);
   const size_t smem = (size_t)p.words_per_team * 4;
-  cudaError_t e = cudaFuncSetAttribute((const void *)fn,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = allow_max_smem((const void *)fn);
   if (e != cudaSuccess) return e;
   if (a.nq == 0) return cudaSuccess;
   fn<<<a.nq, width * 32, smem, stream>>>(g, a, p, width);

@@ -250,7 +250,8 @@ def repair_connectivity(adj: np.ndarray, knn_ids: np.ndarray, ep: int, X: torch.
     id order; each one still unreached gets one in-edge from a reachable node
     with a free slot -- its nearest reachable k-NN neighbour when there is
     one, else the nearest such node by brute force -- and everything it
-    reaches is marked reached.  Existing edges are never replaced."""
+    reaches is marked reached (an incremental search over unreached nodes
+    only).  Existing edges are never replaced."""
     adj = adj.copy()
     n, R = adj.shape
     seen = np.zeros(n, dtype=bool)
@@ -274,9 +275,14 @@ def repair_connectivity(adj: np.ndarray, knn_ids: np.ndarray, ep: int, X: torch.
                 raise RuntimeError("graph repair: no reachable node has a free slot")
         adj[v, deg[v]] = u
         deg[v] += 1
-        g = _csr(adj)
-        from scipy.sparse.csgraph import breadth_first_order
-        seen[breadth_first_order(g, u, directed=True, return_predecessors=False)] = True
+        seen[u] = True
+        stack = [int(u)]
+        while stack:
+            x = stack.pop()
+            for y in adj[x, :deg[x]]:
+                if not seen[y]:
+                    seen[y] = True
+                    stack.append(int(y))
     return adj
 
 

@@ -143,8 +143,8 @@ def test_visited_spill_to_global_bitset(oracle_lib):
     X, Q, adj, ep = _synthetic(5, 20000, 64, 32, 0, clusters=4)
     idx = _index(X, adj, ep, 0)
     o_ids, o_d, ndc, _ = O.search(X, adj, ep, 0, Q, 50, 400)
-    assert ndc.max() > 768  # the smallest hash (1024 slots, 768 before spilling) overflows
-    idx.set_tuning(warps_per_block=4, hash_cap=1024)
+    assert ndc.max() > 1024  # the smallest visited table (512 slots) must overflow
+    idx.set_tuning(warps_per_block=4, hash_cap=512)
     for _ in range(2):  # second pass checks the bitsets were cleared
         ids, d = idx.search_batch(Q, 50, 400)
         assert np.array_equal(ids, o_ids) and _same_bits(d, o_d)
