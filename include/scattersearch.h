@@ -145,6 +145,37 @@ int ss_search_batch_device(ss_index *h, const float *queries, uint32_t nq, const
  * device batch on this handle whose status was nonzero. */
 int ss_batch_status(ss_index *h, uint32_t *failed_queries);
 
+/* Allocation-free batched search.  No counterpart in the reference, which
+ * runs on the host.  It exists for callers that must not allocate device
+ * memory: a process whose device memory belongs to a host framework's pool
+ * allocator with a fixed budget, or a latency-critical serving loop where the
+ * device-wide synchronisation of cudaMalloc/cudaFree would stall other work.
+ * Same search and results as ss_search_batch_device with uniform K and L
+ * (queries, ids, dists are device pointers; dists may be NULL), but it calls
+ * no cudaMalloc, cudaFree or allocating library routine: its scratch (work
+ * queue head, per-query status, per-team visited bitsets) is one static
+ * device array of SS_NOALLOC_SCRATCH_BYTES that every GPU loading the library
+ * holds until the process exits.
+ *   - Limits: nq <= SS_NOALLOC_MAX_QUERIES, and one visited bitset of
+ *     ceil(num/32) words must fit the scratch; beyond them the call fails
+ *     with SS_ERR_UNSUPPORTED before any work.  On large indexes fewer query
+ *     teams fit the scratch, so throughput can be lower than the allocating
+ *     entry points'.
+ *   - The first call on a device sets the scratch up (it resolves the
+ *     array's device address), so make that first call before any stream
+ *     capture begins.
+ *   - Every call, from any handle in the process, shares the one array per
+ *     device and each call clears the parts it uses: calls whose work
+ *     overlaps on the GPU (other streams, other threads) race and must be
+ *     serialised by the caller.
+ *   - Enqueued on `stream` (a cudaStream_t, NULL for the legacy default
+ *     stream); the call returns once the search has finished, reporting
+ *     SS_ERR_SEARCH_LIMIT if any query hit the hop limit. */
+#define SS_NOALLOC_MAX_QUERIES 65536
+#define SS_NOALLOC_SCRATCH_BYTES (16u << 20)
+int ss_search_batch_noalloc(ss_index *h, const float *queries, uint32_t nq, int K, int L,
+                            uint32_t *ids, float *dists, void *stream);
+
 /* Replaces ANNSearch::MultiThreadSearchArraySimulation[WithET]
  * (src/annsearch.cpp:532-699, :839-1025): one query searched by a CTA of
  * `num_threads` warps (1..SS_MAX_INTRA_WIDTH), each step expanding the

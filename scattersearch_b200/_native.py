@@ -20,6 +20,8 @@ STATUS_NAMES = {
 SS_MAX_L = 4096
 SS_MAX_DEGREE = 128
 SS_MAX_INTRA_WIDTH = 16
+SS_NOALLOC_MAX_QUERIES = 65536
+SS_NOALLOC_SCRATCH_BYTES = 16 << 20
 
 # Every function the header declares, with its ctypes signature.
 _vp = ctypes.c_void_p
@@ -45,6 +47,7 @@ SIGNATURES = {
     "ss_search_batch_device": (_i32, [_vp, _vp, _u32, _vp, _vp, _vp, _i32, _i32, _i32, _vp, _vp,
                                       _vp, _vp, _vp]),
     "ss_batch_status": (_i32, [_vp, _u32p]),
+    "ss_search_batch_noalloc": (_i32, [_vp, _vp, _u32, _i32, _i32, _vp, _vp, _vp]),
     "ss_search_intra": (_i32, [_vp, _f32p, _i32, _i32, _i32, _u32p, _f32p]),
     "ss_search_intra_batch": (_i32, [_vp, _f32p, _u32, _i32, _i32, _i32, _u32p, _f32p]),
     "ss_search_intra_batch_device": (_i32, [_vp, _vp, _u32, _i32, _i32, _i32, _vp, _vp, _vp, _vp,

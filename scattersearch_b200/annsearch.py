@@ -250,6 +250,17 @@ class ANNSearch:
             _dptr(dists), _dptr(ndc), _dptr(hops),
             ctypes.c_void_p(int(stream)) if stream else None))
 
+    def search_batch_noalloc(self, queries, nq: int, K: int, L: int, ids, dists=None,
+                             stream=None):
+        """Batched search on device buffers that allocates no device memory
+        (ss_search_batch_noalloc): for callers that must not call cudaMalloc.
+        Its scratch is a fixed static device array shared by every call in
+        the process, so overlapping calls race; returns once the search on
+        ``stream`` has finished."""
+        self._check(self._lib.ss_search_batch_noalloc(
+            self._h, _dptr(queries), int(nq), int(K), int(L), _dptr(ids), _dptr(dists),
+            ctypes.c_void_p(int(stream)) if stream else None))
+
     def batch_status(self) -> int:
         """Failed queries of the last device batch (call after synchronising)."""
         n = ctypes.c_uint32()

@@ -657,6 +657,72 @@ int ss_batch_status(ss_index *h, uint32_t *failed_queries) {
   return SS_OK;
 }
 
+int ss_search_batch_noalloc(ss_index *h, const float *queries, uint32_t nq, int K, int L,
+                            uint32_t *ids, float *dists, void *stream) {
+  int rc = check_search_args(h, K, L);
+  if (rc) return rc;
+  if (nq > SS_NOALLOC_MAX_QUERIES)
+    return set_err(h, SS_ERR_UNSUPPORTED,
+                   "nq=%u exceeds SS_NOALLOC_MAX_QUERIES=%d of the allocation-free search", nq,
+                   SS_NOALLOC_MAX_QUERIES);
+  if (nq == 0) return SS_OK;
+  if (!queries || !ids) return set_err(h, SS_ERR_INVALID_ARGUMENT, "null queries or ids");
+  static_assert(SS_NOALLOC_MAX_QUERIES == ssb::kNoallocMaxQueries, "header and scratch differ");
+  static_assert((size_t)SS_NOALLOC_SCRATCH_BYTES == ssb::kNoallocScratchBytes,
+                "header and scratch differ");
+  DeviceGuard dg(h->device);
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  ssb::GraphView g = h->view();
+  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L, h->hash_cap_override);
+  int wpb = choose_wpb(h, plan);
+  if ((size_t)plan.words_per_team * 4 * wpb > 227 * 1024)
+    return set_err(h, SS_ERR_UNSUPPORTED, "L=%d needs %u bytes of shared memory per query", L,
+                   plan.words_per_team * 4);
+  ssb::NoallocScratch sc{};
+  SS_CUDA(h, ssb::noalloc_scratch(&sc), "allocation-free scratch set-up");
+  // Every resident query team owns one visited bitset of the scratch; the
+  // grid shrinks to the teams whose bitsets fit.
+  const size_t words = spill_words(h);
+  const size_t teams_fit = sc.spill_words / words;
+  if (teams_fit < 1)
+    return set_err(h, SS_ERR_UNSUPPORTED,
+                   "an index of %u nodes needs %zu bytes of visited bitset per query team, more "
+                   "than the %zu-byte scratch of the allocation-free search holds",
+                   h->n, words * 4, sc.spill_words * 4);
+  while (wpb > 1 && (size_t)wpb > teams_fit) wpb >>= 1;
+  int blocks = persistent_blocks(h, plan, wpb, nq);
+  if (blocks <= 0) return set_err(h, SS_ERR_UNSUPPORTED, "search kernel cannot be resident");
+  blocks = (int)std::min<size_t>((size_t)blocks, teams_fit / (size_t)wpb);
+  ssb::BatchArgs a{};
+  a.queries = queries;
+  a.qstride = h->dim;
+  a.nq = nq;
+  a.K0 = K;
+  a.L0 = L;
+  a.ids = ids;
+  a.dists = dists;
+  a.status = sc.status;
+  a.work_counter = sc.counter;
+  a.spill_bits = sc.spill;
+  a.spill_words = (uint32_t)words;
+  a.max_hops = h->n + 1;
+  // The scratch keeps whatever the previous call left: clear the queue head,
+  // the failure count, this batch's status words and the bitsets in use.
+  SS_CUDA(h, cudaMemsetAsync(sc.counter, 0, 2 * sizeof(uint32_t), st), "scratch reset");
+  SS_CUDA(h, cudaMemsetAsync(sc.status, 0, (size_t)nq * 4, st), "scratch reset");
+  SS_CUDA(h, cudaMemsetAsync(sc.spill, 0, (size_t)blocks * wpb * words * 4, st), "scratch reset");
+  SS_CUDA(h, ssb::launch_warp_search(g, a, plan, wpb, blocks, st), "search launch");
+  SS_CUDA(h, ssb::launch_count_failed(sc.status, nq, sc.failed, st), "status count launch");
+  uint32_t failed = 0;
+  SS_CUDA(h, cudaMemcpyAsync(&failed, sc.failed, sizeof(failed), cudaMemcpyDeviceToHost, st),
+          "status count download");
+  SS_CUDA(h, cudaStreamSynchronize(st), "allocation-free search");
+  if (failed)
+    return set_err(h, SS_ERR_SEARCH_LIMIT,
+                   "%u queries hit the hop limit or overflowed the visited table", failed);
+  return SS_OK;
+}
+
 static int intra_common(ss_index *h, const float *queries, uint32_t nq, int K, int L, int W,
                         uint32_t *ids, float *dists) {
   int rc = check_search_args(h, K, L);

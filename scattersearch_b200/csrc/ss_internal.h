@@ -70,4 +70,24 @@ cudaError_t launch_intra_search(const GraphView &g, const BatchArgs &a, const Sm
 // Resident CTAs per SM for the warp kernel with this plan (0 if it cannot run).
 int warp_search_occupancy(const GraphView &g, const SmemPlan &p, int warps_per_block);
 
+// Scratch of the allocation-free batched search: a static device array of
+// kNoallocScratchBytes per GPU (sizes mirrored by SS_NOALLOC_* in
+// include/scattersearch.h).
+constexpr size_t kNoallocScratchBytes = size_t(16) << 20;
+constexpr uint32_t kNoallocMaxQueries = 65536;
+struct NoallocScratch {
+  uint32_t *counter;  // persistent work-queue head
+  uint32_t *failed;   // count of queries with a nonzero status
+  int32_t *status;    // kNoallocMaxQueries entries
+  uint32_t *spill;    // visited bitsets of the query teams
+  size_t spill_words; // capacity of `spill` in words
+};
+// Device addresses of the scratch on the current device.  The first call on
+// a device resolves them (cudaGetSymbolAddress); later calls only read a
+// cache.
+cudaError_t noalloc_scratch(NoallocScratch *out);
+// Adds the number of nonzero status[0..nq) to *failed.
+cudaError_t launch_count_failed(const int32_t *status, uint32_t nq, uint32_t *failed,
+                                cudaStream_t stream);
+
 }  // namespace ssb

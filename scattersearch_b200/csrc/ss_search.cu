@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <mutex>
 #include <set>
 #include <utility>
@@ -1305,6 +1306,71 @@ cudaError_t launch_intra_search(const GraphView &g, const BatchArgs &a, const Sm
   if (e != cudaSuccess) return e;
   if (a.nq == 0) return cudaSuccess;
   fn<<<a.nq, width * 32, smem, stream>>>(g, a, p, width);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------ allocation-free launch ---
+// Scratch of ss_search_batch_noalloc: one file-scope device array per GPU
+// that loads the library, held until the process exits.  Layout (4-byte
+// words): [0] work-queue head, [1] failed-query count, [64, 64 + max
+// queries) per-query status, then the per-team visited bitsets.  Every call
+// shares it, so calls whose work overlaps on the GPU race; each call clears
+// the parts it uses before its search runs.
+namespace {
+constexpr size_t kNoallocWords = kNoallocScratchBytes / 4;
+constexpr size_t kNoallocStatusAt = 64;
+constexpr size_t kNoallocSpillAt =
+    (kNoallocStatusAt + kNoallocMaxQueries + 63) / 64 * 64;  // 256-byte aligned
+static_assert(kNoallocSpillAt < kNoallocWords, "scratch too small for its status words");
+
+static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoallocWords];
+
+// Counts the nonzero statuses of a batch into *failed (zeroed beforehand).
+__global__ void __launch_bounds__(256) count_failed_kernel(const int32_t *status, uint32_t nq,
+                                                           uint32_t *failed) {
+  uint32_t c = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x)
+    c += status[i] != kStatusOk;
+  c = __reduce_add_sync(kFull, c);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(failed, c);
+}
+}  // namespace
+
+cudaError_t noalloc_scratch(NoallocScratch *out) {
+  // Host code cannot use the array's name as a device address (on the host
+  // it names a host-side stand-in), so its device address is resolved once
+  // per device, with that device current, and cached.
+  constexpr int kMaxDevices = 64;
+  static std::mutex mu;
+  static uint32_t *addr[kMaxDevices] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  uint32_t *base = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (!addr[dev]) {
+      void *p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess) return e;
+      addr[dev] = static_cast<uint32_t *>(p);
+    }
+    base = addr[dev];
+  }
+  out->counter = base;
+  out->failed = base + 1;
+  out->status = reinterpret_cast<int32_t *>(base + kNoallocStatusAt);
+  out->spill = base + kNoallocSpillAt;
+  out->spill_words = kNoallocWords - kNoallocSpillAt;
+  return cudaSuccess;
+}
+
+cudaError_t launch_count_failed(const int32_t *status, uint32_t nq, uint32_t *failed,
+                                cudaStream_t stream) {
+  if (nq == 0) return cudaSuccess;
+  const uint32_t blocks = std::min<uint32_t>((nq + 255) / 256, 148);
+  count_failed_kernel<<<blocks, 256, 0, stream>>>(status, nq, failed);
   return cudaGetLastError();
 }
 

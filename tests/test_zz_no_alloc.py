@@ -1,0 +1,110 @@
+"""The allocation-free batched search, ss_search_batch_noalloc.
+
+Some callers cannot call cudaMalloc: a process whose device memory belongs to
+a host framework's pool allocator with a fixed budget, or a serving loop
+that cannot afford the device-wide synchronisation of cudaMalloc/cudaFree.
+For them the library has one entry point whose scratch is a static device
+array instead of an allocation.  These tests call it through the C ABI, on
+device buffers the test owns, and require it to return exactly what the
+allocating entry point ss_search_batch_device returns (identical ids and
+identical float32 distance bits, the bar of every parity test here), on two
+calls in a row, so that contents left in the shared scratch by one call
+cannot leak into the next.
+
+The file name makes pytest collect it last: a run that stops at the first
+failure has run every other test before this one.  It passes on its own in a
+fresh process as well as after the rest of the suite.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import load_fixture
+
+pytestmark = pytest.mark.gpu
+
+
+def _same_bits(a, b):
+    return np.array_equal(np.asarray(a, np.float32).view(np.uint32),
+                          np.asarray(b, np.float32).view(np.uint32))
+
+
+def _noalloc(idx, q, nq, K, L, ids, dists, stream):
+    """One call of the C entry point itself (no Python wrapper in between)."""
+    from scattersearch_b200 import _native
+    lib = _native.lib()
+    return lib.ss_search_batch_noalloc(idx._h, ctypes.c_void_p(q.data_ptr()), nq, K, L,
+                                       ctypes.c_void_p(ids.data_ptr()),
+                                       ctypes.c_void_p(dists.data_ptr()),
+                                       ctypes.c_void_p(stream.cuda_stream))
+
+
+def _compare_two_calls(idx, queries, K, L):
+    import torch
+    nq = len(queries)
+    q = torch.from_numpy(np.ascontiguousarray(queries, np.float32)).cuda()
+    stream = torch.cuda.Stream()
+    ref_ids = torch.empty((nq, K), dtype=torch.int32, device="cuda")
+    ref_d = torch.empty((nq, K), dtype=torch.float32, device="cuda")
+    with torch.cuda.stream(stream):
+        idx.search_batch_device(q, nq, ref_ids, ref_d, K=K, L=L, stream=stream.cuda_stream)
+    stream.synchronize()
+    assert idx.batch_status() == 0
+    ref_ids = ref_ids.cpu().numpy().view(np.uint32)
+    ref_d = ref_d.cpu().numpy()
+    for call in range(2):
+        ids = torch.full((nq, K), -1, dtype=torch.int32, device="cuda")
+        d = torch.full((nq, K), float("nan"), dtype=torch.float32, device="cuda")
+        rc = _noalloc(idx, q, nq, K, L, ids, d, stream)
+        assert rc == 0, idx._lib.ss_last_error(idx._h)
+        assert np.array_equal(ids.cpu().numpy().view(np.uint32), ref_ids), (call, K, L)
+        assert _same_bits(d.cpu().numpy(), ref_d), (call, K, L)
+
+
+def _index(base, adj, ep, metric):
+    from scattersearch_b200 import ANNSearch
+    idx = ANNSearch(base.shape[1], base.shape[0], base, metric)
+    idx.SetGraph(adj, int(ep))
+    return idx
+
+
+@pytest.mark.parametrize("name", ["search_l2_d200", "search_ip_d96"])
+def test_noalloc_matches_allocating_entry_point(name):
+    fx = load_fixture(name)
+    idx = _index(fx["base"], fx["adj"], fx["ep"], int(fx["metric"]))
+    for K, L in ((10, 100), (1, 16)):
+        _compare_two_calls(idx, fx["queries"], K, L)
+    idx.close()
+
+
+def test_noalloc_visited_overflow_uses_the_static_bitsets():
+    """A visited table far smaller than the visited sets makes every query
+    spill into its team's bitset in the static scratch; the second call must
+    find those bitsets cleared."""
+    from scattersearch_b200 import graph
+    rng = np.random.default_rng(5)
+    n, dim = 20000, 64
+    means = rng.standard_normal((4, dim)).astype(np.float32)
+    X = (means[rng.integers(0, 4, n)] + 0.4 * rng.standard_normal((n, dim))).astype(np.float32)
+    Q = (means[rng.integers(0, 4, 128)] + 0.4 * rng.standard_normal((128, dim))).astype(np.float32)
+    adj, ep = graph.build_graph(X, R=32, knn_k=64, device="cpu")
+    idx = _index(X, adj, ep, 0)
+    idx.set_tuning(warps_per_block=4, hash_cap=512)
+    _compare_two_calls(idx, Q, 50, 400)
+    idx.close()
+
+
+def test_noalloc_rejects_batches_beyond_its_scratch():
+    import torch
+    from scattersearch_b200 import _native
+    fx = load_fixture("search_l2_d64")
+    idx = _index(fx["base"], fx["adj"], fx["ep"], 0)
+    q = torch.zeros(8, dtype=torch.float32, device="cuda")
+    out = torch.zeros(8, dtype=torch.int32, device="cuda")
+    rc = _native.lib().ss_search_batch_noalloc(
+        idx._h, ctypes.c_void_p(q.data_ptr()), _native.SS_NOALLOC_MAX_QUERIES + 1, 10, 50,
+        ctypes.c_void_p(out.data_ptr()), None, None)
+    assert rc == 7  # SS_ERR_UNSUPPORTED, before any work is enqueued
+    assert b"SS_NOALLOC_MAX_QUERIES" in idx._lib.ss_last_error(idx._h)
+    idx.close()
