@@ -153,14 +153,11 @@ int ss_batch_status(ss_index *h, uint32_t *failed_queries);
  * Same search and results as ss_search_batch_device with uniform K and L
  * (queries, ids, dists are device pointers; dists may be NULL), but it calls
  * no cudaMalloc, cudaFree or allocating library routine: its scratch (work
- * queue head, per-query status, per-team visited bitsets) is one static
- * device array of SS_NOALLOC_SCRATCH_BYTES that every GPU loading the library
- * holds until the process exits.
- *   - Limits: nq <= SS_NOALLOC_MAX_QUERIES, and one visited bitset of
- *     ceil(num/32) words must fit the scratch; beyond them the call fails
- *     with SS_ERR_UNSUPPORTED before any work.  On large indexes fewer query
- *     teams fit the scratch, so throughput can be lower than the allocating
- *     entry points'.
+ * queue head, failure count, per-query status) is one static device array of
+ * SS_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until the
+ * process exits.
+ *   - Limit: nq <= SS_NOALLOC_MAX_QUERIES; a larger batch fails with
+ *     SS_ERR_UNSUPPORTED before any work is enqueued.
  *   - The first call on a device sets the scratch up (it resolves the
  *     array's device address), so make that first call before any stream
  *     capture begins.
@@ -172,7 +169,7 @@ int ss_batch_status(ss_index *h, uint32_t *failed_queries);
  *     stream); the call returns once the search has finished, reporting
  *     SS_ERR_SEARCH_LIMIT if any query hit the hop limit. */
 #define SS_NOALLOC_MAX_QUERIES 65536
-#define SS_NOALLOC_SCRATCH_BYTES (16u << 20)
+#define SS_NOALLOC_SCRATCH_BYTES (256u + 4u * SS_NOALLOC_MAX_QUERIES)
 int ss_search_batch_noalloc(ss_index *h, const float *queries, uint32_t nq, int K, int L,
                             uint32_t *ids, float *dists, void *stream);
 

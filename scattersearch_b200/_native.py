@@ -21,7 +21,7 @@ SS_MAX_L = 4096
 SS_MAX_DEGREE = 128
 SS_MAX_INTRA_WIDTH = 16
 SS_NOALLOC_MAX_QUERIES = 65536
-SS_NOALLOC_SCRATCH_BYTES = 16 << 20
+SS_NOALLOC_SCRATCH_BYTES = 256 + 4 * SS_NOALLOC_MAX_QUERIES
 
 # Every function the header declares, with its ctypes signature.
 _vp = ctypes.c_void_p

@@ -265,8 +265,6 @@ int launch_batch(ss_index *h, SearchCtx *c, const float *d_q, uint32_t nq, const
   int blocks = persistent ? persistent_blocks(h, plan, wpb, nq)
                           : (int)((nq + (uint32_t)wpb - 1) / (uint32_t)wpb);
   if (blocks <= 0) return set_err(h, SS_ERR_UNSUPPORTED, "search kernel cannot be resident");
-  const size_t slots = (size_t)blocks * wpb;
-  SS_CUDA(h, c->spill.ensure(slots * spill_words(h) * 4, true), "spill bitset allocation");
   SS_CUDA(h, c->status.ensure((size_t)std::max(nq, 1u) * 4), "status allocation");
   SS_CUDA(h, c->counter.ensure(16), "counter allocation");
   ssb::BatchArgs a{};
@@ -284,9 +282,7 @@ int launch_batch(ss_index *h, SearchCtx *c, const float *d_q, uint32_t nq, const
   a.hops = d_hops;
   a.status = c->status.as<int32_t>();
   a.work_counter = persistent ? c->counter.as<uint32_t>() : nullptr;
-  a.spill_bits = c->spill.as<uint32_t>();
-  a.spill_words = spill_words(h);
-  a.max_hops = h->n + 1;
+  a.max_hops = h->n + 1;  // the warp kernel's visited table needs no global memory
   if (persistent) SS_CUDA(h, cudaMemsetAsync(c->counter.p, 0, 4, stream), "counter reset");
   SS_CUDA(h, cudaMemsetAsync(c->status.p, 0, (size_t)nq * 4, stream), "status reset");
   SS_CUDA(h, ssb::launch_warp_search(g, a, plan, wpb, blocks, stream), "search launch");
@@ -674,25 +670,14 @@ int ss_search_batch_noalloc(ss_index *h, const float *queries, uint32_t nq, int 
   const cudaStream_t st = static_cast<cudaStream_t>(stream);
   ssb::GraphView g = h->view();
   ssb::SmemPlan plan = ssb::plan_warp_smem(g, L, h->hash_cap_override);
-  int wpb = choose_wpb(h, plan);
+  const int wpb = choose_wpb(h, plan);
   if ((size_t)plan.words_per_team * 4 * wpb > 227 * 1024)
     return set_err(h, SS_ERR_UNSUPPORTED, "L=%d needs %u bytes of shared memory per query", L,
                    plan.words_per_team * 4);
+  const int blocks = persistent_blocks(h, plan, wpb, nq);
+  if (blocks <= 0) return set_err(h, SS_ERR_UNSUPPORTED, "search kernel cannot be resident");
   ssb::NoallocScratch sc{};
   SS_CUDA(h, ssb::noalloc_scratch(&sc), "allocation-free scratch set-up");
-  // Every resident query team owns one visited bitset of the scratch; the
-  // grid shrinks to the teams whose bitsets fit.
-  const size_t words = spill_words(h);
-  const size_t teams_fit = sc.spill_words / words;
-  if (teams_fit < 1)
-    return set_err(h, SS_ERR_UNSUPPORTED,
-                   "an index of %u nodes needs %zu bytes of visited bitset per query team, more "
-                   "than the %zu-byte scratch of the allocation-free search holds",
-                   h->n, words * 4, sc.spill_words * 4);
-  while (wpb > 1 && (size_t)wpb > teams_fit) wpb >>= 1;
-  int blocks = persistent_blocks(h, plan, wpb, nq);
-  if (blocks <= 0) return set_err(h, SS_ERR_UNSUPPORTED, "search kernel cannot be resident");
-  blocks = (int)std::min<size_t>((size_t)blocks, teams_fit / (size_t)wpb);
   ssb::BatchArgs a{};
   a.queries = queries;
   a.qstride = h->dim;
@@ -703,23 +688,18 @@ int ss_search_batch_noalloc(ss_index *h, const float *queries, uint32_t nq, int 
   a.dists = dists;
   a.status = sc.status;
   a.work_counter = sc.counter;
-  a.spill_bits = sc.spill;
-  a.spill_words = (uint32_t)words;
   a.max_hops = h->n + 1;
   // The scratch keeps whatever the previous call left: clear the queue head,
-  // the failure count, this batch's status words and the bitsets in use.
+  // the failure count and this batch's status words.
   SS_CUDA(h, cudaMemsetAsync(sc.counter, 0, 2 * sizeof(uint32_t), st), "scratch reset");
   SS_CUDA(h, cudaMemsetAsync(sc.status, 0, (size_t)nq * 4, st), "scratch reset");
-  SS_CUDA(h, cudaMemsetAsync(sc.spill, 0, (size_t)blocks * wpb * words * 4, st), "scratch reset");
   SS_CUDA(h, ssb::launch_warp_search(g, a, plan, wpb, blocks, st), "search launch");
   SS_CUDA(h, ssb::launch_count_failed(sc.status, nq, sc.failed, st), "status count launch");
   uint32_t failed = 0;
   SS_CUDA(h, cudaMemcpyAsync(&failed, sc.failed, sizeof(failed), cudaMemcpyDeviceToHost, st),
           "status count download");
   SS_CUDA(h, cudaStreamSynchronize(st), "allocation-free search");
-  if (failed)
-    return set_err(h, SS_ERR_SEARCH_LIMIT,
-                   "%u queries hit the hop limit or overflowed the visited table", failed);
+  if (failed) return set_err(h, SS_ERR_SEARCH_LIMIT, "%u queries hit the hop limit", failed);
   return SS_OK;
 }
 

@@ -72,15 +72,14 @@ int warp_search_occupancy(const GraphView &g, const SmemPlan &p, int warps_per_b
 
 // Scratch of the allocation-free batched search: a static device array of
 // kNoallocScratchBytes per GPU (sizes mirrored by SS_NOALLOC_* in
-// include/scattersearch.h).
-constexpr size_t kNoallocScratchBytes = size_t(16) << 20;
+// include/scattersearch.h): 256 bytes of counters, then one status word per
+// query.
 constexpr uint32_t kNoallocMaxQueries = 65536;
+constexpr size_t kNoallocScratchBytes = 256 + size_t(4) * kNoallocMaxQueries;
 struct NoallocScratch {
   uint32_t *counter;  // persistent work-queue head
   uint32_t *failed;   // count of queries with a nonzero status
   int32_t *status;    // kNoallocMaxQueries entries
-  uint32_t *spill;    // visited bitsets of the query teams
-  size_t spill_words; // capacity of `spill` in words
 };
 // Device addresses of the scratch on the current device.  The first call on
 // a device resolves them (cudaGetSymbolAddress); later calls only read a

@@ -272,24 +272,36 @@ __device__ __forceinline__ bool visited_test(const Visited &v, uint32_t id) {
 }
 
 // ------------------------------------------------------- warp per query ---
-// Visited set of the warp kernel: an exact two-choice bucketed hash in
-// shared memory.  Bucket = 8 slots of 16 bits (one 16-byte row, read with a
-// single LDS.128).  An id is mixed by two multiplications with odd constants
-// modulo 2^B (2^B >= n); each product is a bijection of [0, 2^B), so its high
-// bits (the bucket) plus its low bits (the 16-bit tag) identify the id
-// exactly.  Tags of the second choice carry bit 15, so a tag names both the
-// id and the choice; 0xFFFF marks an empty slot.  When both buckets of an id
-// are full the id goes to the per-team global bitset instead, and from then
-// on every lookup that misses the table also consults the bitset.
+// Visited set of the warp kernel: a two-choice bucketed hash in shared memory
+// that may forget ids but never reports an unvisited id as visited.  Bucket =
+// 8 slots of 16 bits (one 16-byte row, read with a single LDS.128).  An id is
+// mixed by two multiplications with odd constants modulo 2^B (2^B >= n);
+// each product is a bijection of [0, 2^B), so its high bits (the bucket) plus
+// its low bits (the 16-bit tag) identify the id exactly.  Tags of the second
+// choice carry bit 15, so a tag names both the id and the choice; 0xFFFF
+// marks an empty slot.  When both buckets of an id are full, a slot of the
+// first bucket chosen by the id is overwritten: the evicted id is forgotten.
+//
+// Forgetting does not change results.  The acceptance threshold
+// pool[size-1] never increases during a search (accepted candidates are
+// below it, and truncation to L only lowers it).  A forgotten id that is met
+// again is evaluated again, to the same distance bits, and then either
+//   - it is in the pool: the pool holds it under exactly that key, so the
+//     acceptance step finds it in the key's run and drops it; or
+//   - it is not: it was rejected (distance >= the threshold then) or pushed
+//     out by L entries at or below its distance, so its distance is >= the
+//     current threshold and it is rejected again.
+// So a forgetful table only costs extra distance evaluations, and the pool
+// check runs only after the first eviction of a query (`lossy`).
 struct QHash {
   uint4 *bkt;
-  uint32_t bbits, rbits, rmask, bmask;
-  uint32_t *bits;  // global spill bitset (n bits), may be null
-  bool spilled;
+  uint32_t rbits, rmask, bmask;
+  bool lossy;  // an id was evicted (or not recorded) during this query
 };
 
 constexpr uint32_t kMix1 = 0x9E3779B1u;
 constexpr uint32_t kMix2 = 0x7FEB352Du;
+constexpr uint32_t kMix3 = 0x2C1B3C6Du;
 constexpr uint32_t kEmptyTag = 0xFFFFu;
 
 __device__ __forceinline__ void qh_keys(const QHash &h, uint32_t id, uint32_t &b1, uint32_t &t1,
@@ -327,62 +339,45 @@ __device__ __forceinline__ uint4 lds128(const uint4 *p) {
   return v;
 }
 
-// Marks `id` visited.  Returns true when it was not visited before.  The
-// calling lanes of one warp must hold distinct ids.  Sets `full` when the id
-// fit in neither bucket (it was then NOT recorded).
-__device__ __forceinline__ bool qh_insert(const QHash &h, uint32_t id, bool &full) {
+// Looks `id` up and records it; true when it was not found.  The calling
+// lanes of one warp must hold distinct ids.  Sets `evicted` when recording
+// it pushed another id out (or, after repeated lost races, when it was not
+// recorded at all).
+__device__ __forceinline__ bool qh_insert(const QHash &h, uint32_t id, bool &evicted) {
   uint32_t b1, t1, b2, t2;
   qh_keys(h, id, b1, t1, b2, t2);
   unsigned short *slots = reinterpret_cast<unsigned short *>(h.bkt);
-  full = false;
-  for (int attempt = 0; attempt < 17; ++attempt) {
+  for (int attempt = 0; attempt < 8; ++attempt) {
     const uint4 v1 = lds128(h.bkt + b1);
     const uint4 v2 = lds128(h.bkt + b2);
     if (bucket_has(v1, t1) || bucket_has(v2, t2)) return false;
     const uint32_t e1 = bucket_empty(v1), e2 = bucket_empty(v2);
-    if ((e1 | e2) == 0u) {
-      full = true;
-      return false;
+    if ((e1 | e2) != 0u) {
+      const bool use1 = __popc(e1) >= __popc(e2);
+      const uint32_t b = use1 ? b1 : b2, t = use1 ? t1 : t2, e = use1 ? e1 : e2;
+      const uint32_t sl = __ffs(e) - 1;
+      if (atomicCAS(slots + b * 8 + sl, (unsigned short)kEmptyTag, (unsigned short)t) == kEmptyTag)
+        return true;
+    } else {
+      const uint32_t sl = (id * kMix3) >> 29;
+      const uint32_t w = sl < 2 ? v1.x : sl < 4 ? v1.y : sl < 6 ? v1.z : v1.w;
+      const unsigned short old = (unsigned short)(w >> ((sl & 1u) * 16u));
+      if (atomicCAS(slots + b1 * 8 + sl, old, (unsigned short)t1) == old) {
+        evicted = true;
+        return true;
+      }
     }
-    const bool use1 = __popc(e1) >= __popc(e2);
-    const uint32_t b = use1 ? b1 : b2, t = use1 ? t1 : t2, e = use1 ? e1 : e2;
-    const uint32_t s = __ffs(e) - 1;
-    if (atomicCAS(slots + b * 8 + s, (unsigned short)kEmptyTag, (unsigned short)t) == kEmptyTag)
-      return true;
   }
-  full = true;  // unreachable: each failed CAS means a slot was taken
-  return false;
-}
-
-__device__ __forceinline__ bool qh_contains(const QHash &h, uint32_t id) {
-  uint32_t b1, t1, b2, t2;
-  qh_keys(h, id, b1, t1, b2, t2);
-  const uint4 v1 = lds128(h.bkt + b1);
-  const uint4 v2 = lds128(h.bkt + b2);
-  return bucket_has(v1, t1) || bucket_has(v2, t2);
+  evicted = true;  // lost every race for a slot: not recorded, may be met again
+  return true;
 }
 
 // Warp-wide visit of one id per lane (`valid` lanes hold distinct ids).
-// Returns true for ids that were not visited before.  All 32 lanes call it.
+// Returns true for ids not found in the table.  All 32 lanes call it.
 __device__ __forceinline__ bool qh_visit_warp(QHash &h, uint32_t id, bool valid) {
-  bool fresh = false;
-  if (!h.spilled) {
-    bool full = false;
-    if (valid) fresh = qh_insert(h, id, full);
-    const unsigned fm = __ballot_sync(kFull, full);
-    if (fm) {
-      h.spilled = true;
-      if (full && h.bits) {  // not in the table: record it in the bitset (never set before)
-        const uint32_t bit = 1u << (id & 31u);
-        fresh = (atomicOr(h.bits + (id >> 5), bit) & bit) == 0u;
-      }
-    }
-  } else if (valid && h.bits) {
-    if (!qh_contains(h, id)) {
-      const uint32_t bit = 1u << (id & 31u);
-      fresh = (atomicOr(h.bits + (id >> 5), bit) & bit) == 0u;
-    }
-  }
+  bool fresh = false, ev = false;
+  if (valid) fresh = qh_insert(h, id, ev);
+  if (__any_sync(kFull, ev)) h.lossy = true;
   return fresh;
 }
 
@@ -425,8 +420,8 @@ struct WarpSmem {
   float *q;
   uint32_t *pk, *pid;              // pool keys / ids (bit 31 of id = explored)
   uint32_t *cid, *ckey;            // this hop's fresh candidates, adjacency order
-  uint32_t *ak, *aid;              // accepted candidates, adjacency order
-  uint32_t *sk, *sid;              // accepted candidates, sorted
+  uint32_t *ak, *aid, *acle;       // accepted candidates (key, id, pool rank), adjacency order
+  uint32_t *sk, *sid, *scle;       // accepted candidates, sorted by (key, adjacency position)
   uint4 *bkt;                      // visited hash buckets
 };
 
@@ -438,28 +433,23 @@ __device__ __forceinline__ WarpSmem carve_warp(uint32_t *base, const SmemPlan &p
   base += p.pool_cap;
   s.pid = base;
   base += p.pool_cap;
-  s.cid = base;
-  base += p.cand_cap;
-  s.ckey = base;
-  base += p.cand_cap;
-  s.ak = base;
-  base += p.cand_cap;
-  s.aid = base;
-  base += p.cand_cap;
-  s.sk = base;
-  base += p.cand_cap;
-  s.sid = base;
-  base += p.cand_cap;
+  uint32_t **bufs[8] = {&s.cid, &s.ckey, &s.ak, &s.aid, &s.acle, &s.sk, &s.sid, &s.scle};
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    *bufs[i] = base;
+    base += p.cand_cap;
+  }
   s.bkt = reinterpret_cast<uint4 *>(base);
   return s;
 }
 
-// Sorts the n candidates (keys ks[0..n), ids is[0..n), adjacency order) by
-// (key, position) into sk/sid: lane i ranks its candidate by counting the
-// candidates that precede it.  n <= 32*ITEMS.
+// Sorts the n accepted candidates (ks keys, is ids, cs pool ranks, all in
+// adjacency order) by (key, position) into sk/sid/scs: lane i ranks its
+// candidate by counting the candidates that precede it.  n <= 32*ITEMS.
 template <int ITEMS>
-__device__ __forceinline__ void rank_sort(const uint32_t *ks, const uint32_t *is, int n,
-                                          uint32_t *sk, uint32_t *sid, int lane) {
+__device__ __forceinline__ void rank_sort(const uint32_t *ks, const uint32_t *is, const uint32_t *cs,
+                                          int n, uint32_t *sk, uint32_t *sid, uint32_t *scs,
+                                          int lane) {
   uint32_t mk[ITEMS];
   int rank[ITEMS];
 #pragma unroll
@@ -467,6 +457,7 @@ __device__ __forceinline__ void rank_sort(const uint32_t *ks, const uint32_t *is
     mk[t] = (t * 32 + lane) < n ? ks[t * 32 + lane] : 0u;
     rank[t] = 0;
   }
+#pragma unroll 4
   for (int j = 0; j < n; ++j) {
     const uint32_t kj = ks[j];
 #pragma unroll
@@ -481,6 +472,7 @@ __device__ __forceinline__ void rank_sort(const uint32_t *ks, const uint32_t *is
     if (i < n) {
       sk[rank[t]] = mk[t];
       sid[rank[t]] = is[i];
+      scs[rank[t]] = cs[i];
     }
   }
 }
@@ -497,23 +489,32 @@ __device__ __forceinline__ void load_row(const GraphView &g, uint32_t node, int 
   }
 }
 
+// Starts an L2 prefetch of a node's adjacency row (one lane issues it).
+__device__ __forceinline__ void prefetch_adj_l2(const GraphView &g, uint32_t node) {
+  const uint32_t *nrow = g.adj + (size_t)node * g.rstride;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(nrow), "r"(g.rstride * 4u)
+               : "memory");
+}
+
 // One query, one warp.  Each hop (batch-merge form of annsearch.cpp:218-253):
-//   1. expand the first unexplored pool slot (all slots before `cursor` are
-//      explored);
-//   2. read its adjacency row; drop ids already visited and mark the rest
+//   1. expand the first unexplored pool slot k (all slots before `cursor` are
+//      explored); u is the unexplored slot after it;
+//   2. read k's adjacency row; drop ids already visited and mark the rest
 //      visited, the first occurrence in adjacency order winning (:229-231);
 //   3. compute their distances (:236);
-//   4. accept d < pool[size-1] taken at the start of the hop (:238);
+//   4. accept d < pool[size-1] taken at the start of the hop (:238); each
+//      accepted key's rank in the pool (entries <= key) is its merge offset;
 //   5. sort accepted candidates by (d, adjacency position) and stable-merge
 //      them into the pool, older entries first on ties, truncated to L
 //      (InsertIntoPool upper-bound insert, util.h:56-75; :242-243).
-// The adjacency row of the hop after this one is loaded while the merge runs.
+// The next expansion is known after step 4 (u, unless the best accepted
+// candidate lands before it), so its adjacency row is loaded while step 5
+// runs; u's row is also sent to L2 at the start of the hop.
 template <int NB, int RCH>
 __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qsrc, int K, int L,
                                 uint32_t *out_ids, float *out_dists, uint32_t *out_ndc,
                                 uint32_t *out_hops, int32_t *out_status, const WarpSmem &s,
-                                const SmemPlan &p, uint32_t *spill, uint32_t spill_words,
-                                uint32_t max_hops, int lane) {
+                                const SmemPlan &p, uint32_t max_hops, int lane) {
   const unsigned lanemask_lt = (1u << lane) - 1u;
   const int qw = (int)g.nb * 8;
   for (int i = lane; i < qw; i += 32) s.q[i] = i < (int)g.dim ? qsrc[i] : 0.f;
@@ -523,12 +524,10 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
 
   QHash vis;
   vis.bkt = s.bkt;
-  vis.bbits = p.hash_log2;
   vis.rbits = p.qh_rbits;
   vis.rmask = (1u << p.qh_rbits) - 1u;
   vis.bmask = (p.hash_log2 + p.qh_rbits >= 32) ? ~0u : ((1u << (p.hash_log2 + p.qh_rbits)) - 1u);
-  vis.bits = spill;
-  vis.spilled = false;
+  vis.lossy = false;
 
   uint32_t ndc = 0, hops = 0;
   int32_t status = kStatusOk;
@@ -554,7 +553,7 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
     eval_all<NB>(g, s.q, s.cid, s.ckey, size, lane);
     ndc += size;
     __syncwarp();
-    rank_sort<RCH>(s.ckey, s.cid, size, s.pk, s.pid, lane);
+    rank_sort<RCH>(s.ckey, s.cid, s.cid, size, s.pk, s.pid, s.sid, lane);
     __syncwarp();
   }
 
@@ -567,14 +566,18 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
 
   int cursor = 0;
   for (;;) {
-    // 1. first unexplored slot at or after the cursor
-    int k = -1;
+    // 1. first two unexplored slots at or after the cursor
+    int k = -1, u = -1;
     for (int b0 = cursor; b0 < size; b0 += 32) {
       const int idx = b0 + lane;
       const bool un = idx < size && !(s.pid[idx] & kExplored);
-      const unsigned bm = __ballot_sync(kFull, un);
-      if (bm) {
+      unsigned bm = __ballot_sync(kFull, un);
+      if (k < 0 && bm) {
         k = b0 + __ffs(bm) - 1;
+        bm &= bm - 1u;
+      }
+      if (bm) {
+        u = b0 + __ffs(bm) - 1;
         break;
       }
     }
@@ -585,8 +588,12 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
     }
     const uint32_t node = s.pid[k];
     const uint32_t thr = s.pk[size - 1];
+    const uint32_t unode = u >= 0 ? (s.pid[u] & ~kExplored) : kNoneId;
     __syncwarp();
-    if (lane == 0) s.pid[k] = node | kExplored;
+    if (lane == 0) {
+      s.pid[k] = node | kExplored;
+      if (unode != kNoneId) prefetch_adj_l2(g, unode);
+    }
     ++hops;
     uint32_t row[RCH];
     if (node == pref_node) {
@@ -608,12 +615,10 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
       if (fresh) s.cid[nc + __popc(fm & lanemask_lt)] = row[c];
       nc += __popc(fm);
     }
-    if (vis.spilled && !spill) {
-      status = kStatusVisitedFull;
-      break;
-    }
     if (nc == 0) {
-      pref_node = kNoneId;
+      pref_node = unode;
+      if (unode != kNoneId) load_row<RCH>(g, unode, lane, pref_row);
+      cursor = k + 1;
       continue;
     }
     __syncwarp();
@@ -623,47 +628,81 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
     ndc += nc;
     __syncwarp();
 
-    // 4. acceptance (adjacency order), then rank sort by (key, m)
+    // 4. acceptance in adjacency order, with each key's pool rank; after an
+    //    eviction, a candidate already in the pool (same id under the same
+    //    key) is dropped
+    const int top = floor_pow2(size);
     int na = 0;
 #pragma unroll
     for (int c = 0; c < RCH; ++c) {
       const int e = c * 32 + lane;
       const uint32_t key = e < nc ? s.ckey[e] : 0xFFFFFFFFu;
-      const bool acc = e < nc && key < thr;
+      bool acc = e < nc && key < thr;
+      int cle = 0;
+      uint32_t id = 0;
+      if (acc) {
+        id = s.cid[e];
+        cle = count_le_bf(s.pk, size, top, key);
+        if (vis.lossy) {
+          for (int j = cle - 1; j >= 0 && s.pk[j] == key; --j) {
+            if ((s.pid[j] & ~kExplored) == id) {
+              acc = false;
+              break;
+            }
+          }
+        }
+      }
       const unsigned am = __ballot_sync(kFull, acc);
       if (acc) {
         const int pos = na + __popc(am & lanemask_lt);
         s.ak[pos] = key;
-        s.aid[pos] = s.cid[e];
+        s.aid[pos] = id;
+        s.acle[pos] = (uint32_t)cle;
       }
       na += __popc(am);
     }
-    // next pick if nothing is accepted: first unexplored after k
-    int u = -1;
-    for (int b0 = k + 1; b0 < size; b0 += 32) {
-      const int idx = b0 + lane;
-      const bool un = idx < size && !(s.pid[idx] & kExplored);
-      const unsigned bm = __ballot_sync(kFull, un);
-      if (bm) {
-        u = b0 + __ffs(bm) - 1;
-        break;
-      }
-    }
     if (na == 0) {
-      pref_node = kNoneId;
-      if (u >= 0) {
-        pref_node = s.pid[u];
-        load_row<RCH>(g, pref_node, lane, pref_row);
-      }
+      pref_node = unode;
+      if (unode != kNoneId) load_row<RCH>(g, unode, lane, pref_row);
       cursor = k + 1;
       continue;
     }
     __syncwarp();
-    rank_sort<RCH>(s.ak, s.aid, na, s.sk, s.sid, lane);
+
+    // Next expansion: the best accepted candidate (smallest key, then first
+    // in adjacency order) lands at p0 = its pool rank; old slot u stays ahead
+    // of it iff u < p0.  Its adjacency row loads during the sort and merge.
+    int p0;
+    {
+      uint32_t bk = 0xFFFFFFFFu;
+      int be = 0x7FFFFFFF;
+#pragma unroll
+      for (int c = 0; c < RCH; ++c) {
+        const int e = c * 32 + lane;
+        if (e < na) {
+          const uint32_t kk = s.ak[e];
+          if (kk < bk) {
+            bk = kk;
+            be = e;
+          }
+        }
+      }
+      const uint32_t kmin = __reduce_min_sync(kFull, bk);
+      const int emin = (int)__reduce_min_sync(kFull, bk == kmin ? (uint32_t)be : 0x7FFFFFFFu);
+      p0 = (int)s.acle[emin];
+      const uint32_t nxt = (u >= 0 && u < p0) ? unode : s.aid[emin];
+      pref_node = nxt;
+      load_row<RCH>(g, nxt, lane, pref_row);
+    }
+
+    rank_sort<RCH>(s.ak, s.aid, s.acle, na, s.sk, s.sid, s.scle, lane);
     __syncwarp();
 
-    // 5. stable merge into the pool, in place
-    const int top = floor_pow2(size);
+    // 5. stable merge into the pool, in place.  New entry e (sorted rank)
+    //    goes to e + its pool rank; old entries at and after p0 move up by
+    //    the number of new keys below them, in 128-entry windows from the top
+    //    down, 4 entries per lane, each window fully read before it is
+    //    written.
     uint32_t nkey[RCH], nid[RCH];
     int npos[RCH];
 #pragma unroll
@@ -673,24 +712,9 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
       if (e < na) {
         nkey[c] = s.sk[e];
         nid[c] = s.sid[e];
-        npos[c] = e + count_le_bf(s.pk, size, top, nkey[c]);
+        npos[c] = e + (int)s.scle[e];
       }
     }
-    const int p0 = __shfl_sync(kFull, npos[0], 0);
-    // Prefetch the adjacency row of the next expansion: the old pool's
-    // first unexplored slot after k if it precedes the first new entry,
-    // else the first new entry (when it survives truncation).
-    {
-      uint32_t nxt = kNoneId;
-      if (u >= 0 && u < p0) nxt = s.pid[u];
-      else if (p0 < L) nxt = s.sid[0];
-      else if (u >= 0) nxt = s.pid[u];
-      pref_node = nxt;
-      if (nxt != kNoneId) load_row<RCH>(g, nxt, lane, pref_row);
-    }
-    // Old entries at and after p0 move up by the number of new keys below
-    // them; 128-entry windows from the top down, 4 entries per lane, each
-    // window fully read before it is written.
     for (int w = ((size - 1) >> 7) << 7; w + 128 > p0 && w >= 0; w -= 128) {
       const int j0 = w + 4 * lane;
       const bool any = j0 + 3 >= p0 && j0 < size;
@@ -744,9 +768,6 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
     out_ids[i] = have ? (s.pid[i] & ~kExplored) : 0u;
     if (out_dists) out_dists[i] = have ? key_to_float(s.pk[i]) : 0.f;
   }
-  if (vis.spilled && spill) {
-    for (uint32_t w = lane; w < spill_words; w += 32) spill[w] = 0u;
-  }
   if (lane == 0) {
     if (out_ndc) *out_ndc = ndc;
     if (out_hops) *out_hops = hops;
@@ -755,15 +776,16 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
   __syncwarp();
 }
 
+// At most 128 registers a thread (two 256-thread CTAs' worth per SM): whole
+// rows stay in flight per lane pair and up to 16 query teams fit an SM.
 template <int NB, int RCH>
-__global__ void __launch_bounds__(256) warp_search_kernel(GraphView g, BatchArgs a, SmemPlan p) {
+__global__ void __launch_bounds__(256, 2) warp_search_kernel(GraphView g, BatchArgs a, SmemPlan p) {
   extern __shared__ __align__(16) uint32_t smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wpb = blockDim.x >> 5;
   const WarpSmem s = carve_warp(smem + (size_t)warp * p.words_per_team, p);
   const uint32_t slot = blockIdx.x * wpb + warp;
   const uint32_t nslots = gridDim.x * wpb;
-  uint32_t *spill = a.spill_bits ? a.spill_bits + (size_t)slot * a.spill_words : nullptr;
   uint32_t q = slot;
   for (;;) {
     if (a.work_counter) {
@@ -781,7 +803,7 @@ __global__ void __launch_bounds__(256) warp_search_kernel(GraphView g, BatchArgs
       warp_search_one<NB, RCH>(g, a.queries + (size_t)q * a.qstride, K, L, a.ids + off,
                                a.dists ? a.dists + off : nullptr, a.ndc ? a.ndc + q : nullptr,
                                a.hops ? a.hops + q : nullptr, a.status ? a.status + q : nullptr, s,
-                               p, spill, a.spill_words, a.max_hops, lane);
+                               p, a.max_hops, lane);
     }
     if (!a.work_counter) q += nslots;
   }
@@ -1227,7 +1249,7 @@ SmemPlan plan_warp_smem(const GraphView &g, int L_max, int hash_cap_override) {
   p.qh_rbits = nbits > bbits ? nbits - bbits : 0;
   p.hash_cap = (1u << bbits) * 8;
   p.hash_limit = p.hash_cap;
-  p.words_per_team = p.q_words + 2 * p.pool_cap + 6 * p.cand_cap + (1u << bbits) * 4;
+  p.words_per_team = p.q_words + 2 * p.pool_cap + 8 * p.cand_cap + (1u << bbits) * 4;
   p.words_per_team = round_up(p.words_per_team, 4);
   return p;
 }
@@ -1313,15 +1335,14 @@ cudaError_t launch_intra_search(const GraphView &g, const BatchArgs &a, const Sm
 // Scratch of ss_search_batch_noalloc: one file-scope device array per GPU
 // that loads the library, held until the process exits.  Layout (4-byte
 // words): [0] work-queue head, [1] failed-query count, [64, 64 + max
-// queries) per-query status, then the per-team visited bitsets.  Every call
-// shares it, so calls whose work overlaps on the GPU race; each call clears
-// the parts it uses before its search runs.
+// queries) per-query status.  Every call shares it, so calls whose work
+// overlaps on the GPU race; each call clears the parts it uses before its
+// search runs.
 namespace {
 constexpr size_t kNoallocWords = kNoallocScratchBytes / 4;
 constexpr size_t kNoallocStatusAt = 64;
-constexpr size_t kNoallocSpillAt =
-    (kNoallocStatusAt + kNoallocMaxQueries + 63) / 64 * 64;  // 256-byte aligned
-static_assert(kNoallocSpillAt < kNoallocWords, "scratch too small for its status words");
+static_assert(kNoallocStatusAt + kNoallocMaxQueries <= kNoallocWords,
+              "scratch too small for its status words");
 
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoallocWords];
 
@@ -1361,8 +1382,6 @@ cudaError_t noalloc_scratch(NoallocScratch *out) {
   out->counter = base;
   out->failed = base + 1;
   out->status = reinterpret_cast<int32_t *>(base + kNoallocStatusAt);
-  out->spill = base + kNoallocSpillAt;
-  out->spill_words = kNoallocWords - kNoallocSpillAt;
   return cudaSuccess;
 }
 

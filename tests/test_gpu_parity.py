@@ -137,8 +137,9 @@ def test_synthetic_shapes(oracle_lib, dim, R, metric):
 
 
 def test_visited_spill_to_global_bitset(oracle_lib):
-    """A visited hash far smaller than the query's visited set forces the
-    overflow into the global bitset; results must not change."""
+    """A visited table far smaller than the query's visited set: the warp
+    kernel's table forgets ids (they are evaluated again) and the CTA
+    kernel's overflows into its global bitset; results must not change."""
     O = oracle_lib
     X, Q, adj, ep = _synthetic(5, 20000, 64, 32, 0, clusters=4)
     idx = _index(X, adj, ep, 0)

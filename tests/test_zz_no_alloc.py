@@ -78,10 +78,10 @@ def test_noalloc_matches_allocating_entry_point(name):
     idx.close()
 
 
-def test_noalloc_visited_overflow_uses_the_static_bitsets():
+def test_noalloc_with_a_forgetful_visited_table():
     """A visited table far smaller than the visited sets makes every query
-    spill into its team's bitset in the static scratch; the second call must
-    find those bitsets cleared."""
+    forget visited ids and evaluate them again; results must still match the
+    allocating entry point's, call after call."""
     from scattersearch_b200 import graph
     rng = np.random.default_rng(5)
     n, dim = 20000, 64
