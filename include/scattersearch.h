@@ -198,8 +198,10 @@ int ss_search_intra_batch_device(ss_index *h, const float *queries, uint32_t nq,
  * autotuner (scattersearch_b200.autotune) per (dim, degree, L); no
  * counterpart in the reference, whose only knobs are #defines and argv.
  * warps_per_block: query teams per CTA (1, 2, 4 or 8; 0 = the count that
- * keeps the most teams resident); hash_cap: visited-hash slots per query
- * (0 = automatic, 20 x L rounded up to a power of two);
+ * keeps the most teams resident); hash_cap: visited-table slots per query
+ * (0 = automatic: 2 x L rounded up to a power of two, at least 1024; the
+ * table may forget visited ids, which costs repeated distance evaluations
+ * but never changes results);
  * blocks_per_sm_cap: limit on resident CTAs per SM (0 = occupancy limit). */
 int ss_set_tuning(ss_index *h, int warps_per_block, int hash_cap, int blocks_per_sm_cap);
 

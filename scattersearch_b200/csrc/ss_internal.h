@@ -48,11 +48,19 @@ struct SmemPlan {
   uint32_t qh_rbits;    // warp kernel: tag remainder bits of the visited hash
   uint32_t step_cap;    // CTA kernel: step-local dedupe table (power of two)
   uint32_t step_log2;
+  uint32_t stage_rows;  // warp kernel: rows of the shared-memory row stage
+  uint32_t stage_words; // warp kernel: size of the row stage
   uint32_t words_per_team;
 };
 
 // Query status codes written to BatchArgs::status.
-enum : int32_t { kStatusOk = 0, kStatusBadArgs = 1, kStatusHopLimit = 2, kStatusVisitedFull = 3 };
+enum : int32_t {
+  kStatusOk = 0,
+  kStatusBadArgs = 1,
+  kStatusHopLimit = 2,
+  kStatusVisitedFull = 3,
+  kStatusStageTimeout = 4  // a shared-memory row stage was not filled within its wait limit
+};
 
 // Plans shared memory for a warp-per-query launch.
 SmemPlan plan_warp_smem(const GraphView &g, int L_max, int hash_cap_override);

@@ -33,6 +33,12 @@ namespace {
 constexpr uint32_t kExplored = 0x80000000u;
 constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr uint64_t kInvalidKey = ~0ull;
+// Most rows staged in shared memory per pass of the warp kernel (one per
+// lane pair), and the iteration limit of a wait for them (a stage load takes
+// microseconds; the limit is far above that and only ends a wait that would
+// never finish).
+constexpr int kStageRows = 16;
+constexpr uint32_t kStageWaitLimit = 1u << 24;
 
 // ---------------------------------------------------------------- keys ---
 // Order-preserving map float -> uint32 (ascending).  -0 is folded onto +0 so
@@ -302,7 +308,6 @@ struct QHash {
 constexpr uint32_t kMix1 = 0x9E3779B1u;
 constexpr uint32_t kMix2 = 0x7FEB352Du;
 constexpr uint32_t kMix3 = 0x2C1B3C6Du;
-constexpr uint32_t kEmptyTag = 0xFFFFu;
 
 __device__ __forceinline__ void qh_keys(const QHash &h, uint32_t id, uint32_t &b1, uint32_t &t1,
                                         uint32_t &b2, uint32_t &t2) {
@@ -339,46 +344,47 @@ __device__ __forceinline__ uint4 lds128(const uint4 *p) {
   return v;
 }
 
-// Looks `id` up and records it; true when it was not found.  The calling
-// lanes of one warp must hold distinct ids.  Sets `evicted` when recording
-// it pushed another id out (or, after repeated lost races, when it was not
-// recorded at all).
-__device__ __forceinline__ bool qh_insert(const QHash &h, uint32_t id, bool &evicted) {
+// One lane's probe of the table: both candidate buckets of an id as they
+// were read, and the id's tags in them.
+struct QProbe {
   uint32_t b1, t1, b2, t2;
-  qh_keys(h, id, b1, t1, b2, t2);
-  unsigned short *slots = reinterpret_cast<unsigned short *>(h.bkt);
-  for (int attempt = 0; attempt < 8; ++attempt) {
-    const uint4 v1 = lds128(h.bkt + b1);
-    const uint4 v2 = lds128(h.bkt + b2);
-    if (bucket_has(v1, t1) || bucket_has(v2, t2)) return false;
-    const uint32_t e1 = bucket_empty(v1), e2 = bucket_empty(v2);
-    if ((e1 | e2) != 0u) {
-      const bool use1 = __popc(e1) >= __popc(e2);
-      const uint32_t b = use1 ? b1 : b2, t = use1 ? t1 : t2, e = use1 ? e1 : e2;
-      const uint32_t sl = __ffs(e) - 1;
-      if (atomicCAS(slots + b * 8 + sl, (unsigned short)kEmptyTag, (unsigned short)t) == kEmptyTag)
-        return true;
-    } else {
-      const uint32_t sl = (id * kMix3) >> 29;
-      const uint32_t w = sl < 2 ? v1.x : sl < 4 ? v1.y : sl < 6 ? v1.z : v1.w;
-      const unsigned short old = (unsigned short)(w >> ((sl & 1u) * 16u));
-      if (atomicCAS(slots + b1 * 8 + sl, old, (unsigned short)t1) == old) {
-        evicted = true;
-        return true;
-      }
-    }
-  }
-  evicted = true;  // lost every race for a slot: not recorded, may be met again
-  return true;
+  uint4 v1, v2;
+};
+
+// Read-only lookup; true when `id` is in the table.
+__device__ __forceinline__ bool qh_lookup(const QHash &h, uint32_t id, QProbe &pr) {
+  qh_keys(h, id, pr.b1, pr.t1, pr.b2, pr.t2);
+  pr.v1 = lds128(h.bkt + pr.b1);
+  pr.v2 = lds128(h.bkt + pr.b2);
+  return bucket_has(pr.v1, pr.t1) || bucket_has(pr.v2, pr.t2);
 }
 
-// Warp-wide visit of one id per lane (`valid` lanes hold distinct ids).
-// Returns true for ids not found in the table.  All 32 lanes call it.
-__device__ __forceinline__ bool qh_visit_warp(QHash &h, uint32_t id, bool valid) {
-  bool fresh = false, ev = false;
-  if (valid) fresh = qh_insert(h, id, ev);
+// Records the ids of the `ins` lanes (distinct ids, none found by their
+// qh_lookup, whose bucket reads are still current).  Each id goes to the
+// emptier of its two buckets; lanes that picked the same bucket take its
+// empty slots in lane order, and a lane left without one overwrites a slot
+// chosen by its id, so the table forgets an id.  Plain 16-bit stores, no
+// atomics.  All 32 lanes call it.
+__device__ __forceinline__ void qh_record(QHash &h, const QProbe &pr, uint32_t id, bool ins,
+                                          int lane) {
+  const uint32_t e1 = bucket_empty(pr.v1), e2 = bucket_empty(pr.v2);
+  const bool use1 = __popc(e1) >= __popc(e2);
+  const uint32_t b = use1 ? pr.b1 : pr.b2, t = use1 ? pr.t1 : pr.t2, e = use1 ? e1 : e2;
+  const unsigned grp = __match_any_sync(kFull, ins ? b : (0x80000000u | (uint32_t)lane));
+  const int r = __popc(grp & ((1u << lane) - 1u));
+  unsigned short *slots = reinterpret_cast<unsigned short *>(h.bkt);
+  bool ev = false;
+  if (ins) {
+    uint32_t sl;
+    if (r < __popc(e)) {
+      sl = __fns(e, 0, r + 1);
+    } else {
+      sl = (id * kMix3) >> 29;
+      ev = true;
+    }
+    slots[b * 8 + sl] = (unsigned short)t;
+  }
   if (__any_sync(kFull, ev)) h.lossy = true;
-  return fresh;
 }
 
 // Starts an L2 prefetch of the base rows of cid[0..nc) (one bulk prefetch
@@ -392,14 +398,6 @@ __device__ __forceinline__ void prefetch_rows(const GraphView &g, const uint32_t
     const float *row = g.base + (size_t)cid[e] * (size_t)(g.nb * 8);
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(row), "r"(bytes) : "memory");
   }
-}
-
-// Keys of cid[0..nc) into ckey[0..nc): prefetch every row, then 16 per pass.
-template <int NB>
-__device__ __forceinline__ void eval_all(const GraphView &g, const float *qs, const uint32_t *cid,
-                                         uint32_t *ckey, int nc, int lane) {
-  if (nc > 16) prefetch_rows(g, cid, nc, lane);
-  eval_candidates<NB>(g, qs, cid, ckey, nc, lane);
 }
 
 // Branch-free binary searches over ascending arrays (warp-uniform trip
@@ -416,26 +414,34 @@ __device__ __forceinline__ int count_le_bf(const uint32_t *a, int n, int top, ui
 
 __device__ __forceinline__ int floor_pow2(int n) { return n > 0 ? 1 << (31 - __clz(n)) : 0; }
 
+// Per-team shared memory of the warp kernel.  The row stage comes first so
+// that it starts on a 128-byte boundary (every team's region is a multiple of
+// 128 bytes).
 struct WarpSmem {
+  float *stage;                    // stage_rows base rows (nb*8 floats each), filled by TMA
+  uint64_t *bar;                   // mbarrier of the stage
   float *q;
   uint32_t *pk, *pid;              // pool keys / ids (bit 31 of id = explored)
   uint32_t *cid, *ckey;            // this hop's fresh candidates, adjacency order
   uint32_t *ak, *aid, *acle;       // accepted candidates (key, id, pool rank), adjacency order
-  uint32_t *sk, *sid, *scle;       // accepted candidates, sorted by (key, adjacency position)
   uint4 *bkt;                      // visited hash buckets
 };
 
 __device__ __forceinline__ WarpSmem carve_warp(uint32_t *base, const SmemPlan &p) {
   WarpSmem s;
+  s.stage = reinterpret_cast<float *>(base);
+  base += p.stage_words;
+  s.bar = reinterpret_cast<uint64_t *>(base);
+  base += 4;
   s.q = reinterpret_cast<float *>(base);
   base += p.q_words;
   s.pk = base;
   base += p.pool_cap;
   s.pid = base;
   base += p.pool_cap;
-  uint32_t **bufs[8] = {&s.cid, &s.ckey, &s.ak, &s.aid, &s.acle, &s.sk, &s.sid, &s.scle};
+  uint32_t **bufs[5] = {&s.cid, &s.ckey, &s.ak, &s.aid, &s.acle};
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
+  for (int i = 0; i < 5; ++i) {
     *bufs[i] = base;
     base += p.cand_cap;
   }
@@ -443,38 +449,135 @@ __device__ __forceinline__ WarpSmem carve_warp(uint32_t *base, const SmemPlan &p
   return s;
 }
 
-// Sorts the n accepted candidates (ks keys, is ids, cs pool ranks, all in
-// adjacency order) by (key, position) into sk/sid/scs: lane i ranks its
-// candidate by counting the candidates that precede it.  n <= 32*ITEMS.
-template <int ITEMS>
-__device__ __forceinline__ void rank_sort(const uint32_t *ks, const uint32_t *is, const uint32_t *cs,
-                                          int n, uint32_t *sk, uint32_t *sid, uint32_t *scs,
-                                          int lane) {
-  uint32_t mk[ITEMS];
-  int rank[ITEMS];
-#pragma unroll
-  for (int t = 0; t < ITEMS; ++t) {
-    mk[t] = (t * 32 + lane) < n ? ks[t * 32 + lane] : 0u;
-    rank[t] = 0;
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Bounded wait for phase `parity` of a shared-memory mbarrier; false when the
+// iteration limit ran out first.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (uint32_t spin = 0; spin < kStageWaitLimit; ++spin) {
+    uint32_t done;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
   }
+  return false;
+}
+
+// Row stage of one team: base rows are copied whole into shared memory by
+// the bulk-copy (TMA) engine, one cp.async.bulk per row, completing on the
+// team's mbarrier.  A row requested as one 16-byte-aligned block reaches
+// DRAM as one burst per row, which a random gather needs to approach the
+// HBM copy rate; rows read by many lanes a sector at a time do not.
+struct RowStage {
+  uint32_t bar;     // shared address of the mbarrier
+  uint32_t phase;   // parity of the phase being filled
+  bool broken;      // a wait timed out: the stage may still be written to
+};
+
+// Starts copying the base rows of cid[0..m) (m <= the stage's rows) into the
+// stage.  All 32 lanes call it; cid must be visible to every lane.
+__device__ __forceinline__ void stage_issue(const GraphView &g, const WarpSmem &s, const RowStage &st,
+                                            const uint32_t *cid, int m, int lane) {
+  const uint32_t bytes = g.nb * 32u;
+  // earlier reads of the stage (generic proxy) come before the copies that
+  // overwrite it (async proxy)
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if (lane == 0)
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(st.bar),
+                 "r"(bytes * (uint32_t)m)
+                 : "memory");
+  __syncwarp();
+  if (lane < m) {
+    const float *src = g.base + (size_t)cid[lane] * (size_t)(g.nb * 8);
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(s.stage + lane * (g.nb * 8))),
+        "l"(src), "r"(bytes), "r"(st.bar)
+        : "memory");
+  }
+}
+
+// Waits for the copies of stage_issue.  Returns false on a timed-out wait.
+__device__ __forceinline__ bool stage_wait(RowStage &st) {
+  const bool ok = mbar_wait(st.bar, st.phase);
+  st.phase ^= 1u;
+  if (!ok) st.broken = true;
+  return __all_sync(kFull, ok);
+}
+
+// Distance between the query and staged row `c`, computed by a lane pair:
+// lane h (0/1) of the pair owns reference lanes 4h..4h+3 (the arithmetic of
+// pair_distance, with both operands in shared memory).
+template <int NB>
+__device__ __forceinline__ float staged_distance(const GraphView &g, const float *qs,
+                                                 const float *row, int h) {
+  const int nb = NB > 0 ? NB : (int)g.nb;
+  const float4 *r4 = reinterpret_cast<const float4 *>(row) + h;
+  const float4 *q4 = reinterpret_cast<const float4 *>(qs) + h;
+  float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+  const bool l2 = g.metric == 0;
+  if constexpr (NB > 0) {
+    if (l2) {
+#pragma unroll
+      for (int t = 0; t < NB; ++t) {
+        const int b = block_at(t, NB);
+        acc_l2(a0, a1, a2, a3, q4[2 * b], r4[2 * b]);
+      }
+    } else {
+#pragma unroll
+      for (int t = 0; t < NB; ++t) {
+        const int b = block_at(t, NB);
+        acc_ip(a0, a1, a2, a3, q4[2 * b], r4[2 * b]);
+      }
+    }
+  } else {
 #pragma unroll 4
-  for (int j = 0; j < n; ++j) {
-    const uint32_t kj = ks[j];
-#pragma unroll
-    for (int t = 0; t < ITEMS; ++t) {
-      const int i = t * 32 + lane;
-      rank[t] += (kj < mk[t]) || (kj == mk[t] && j < i);
+    for (int t = 0; t < nb; ++t) {
+      const int b = block_at(t, nb);
+      if (l2) acc_l2(a0, a1, a2, a3, q4[2 * b], r4[2 * b]);
+      else acc_ip(a0, a1, a2, a3, q4[2 * b], r4[2 * b]);
     }
   }
-#pragma unroll
-  for (int t = 0; t < ITEMS; ++t) {
-    const int i = t * 32 + lane;
-    if (i < n) {
-      sk[rank[t]] = mk[t];
-      sid[rank[t]] = is[i];
-      scs[rank[t]] = cs[i];
-    }
+  const float o0 = __shfl_xor_sync(kFull, a0, 1);
+  const float o1 = __shfl_xor_sync(kFull, a1, 1);
+  const float o2 = __shfl_xor_sync(kFull, a2, 1);
+  const float o3 = __shfl_xor_sync(kFull, a3, 1);
+  const float l0 = h ? o0 : a0, l1 = h ? o1 : a1, l2v = h ? o2 : a2, l3 = h ? o3 : a3;
+  const float u0 = h ? a0 : o0, u1 = h ? a1 : o1, u2 = h ? a2 : o2, u3 = h ? a3 : o3;
+  float r = __fadd_rn(l0, l1);
+  r = __fadd_rn(r, l2v);
+  r = __fadd_rn(r, l3);
+  r = __fadd_rn(r, u0);
+  r = __fadd_rn(r, u1);
+  r = __fadd_rn(r, u2);
+  r = __fadd_rn(r, u3);
+  return l2 ? r : -r;
+}
+
+// Keys of cid[0..nc) into ckey[0..nc): rows beyond the first stage load are
+// sent to L2 first, then stage loads of `srows` rows (<= 16), one distance
+// per lane pair.  When `first_issued`, the first load was already started
+// with stage_issue.  Returns false when a stage wait timed out.
+template <int NB>
+__device__ __forceinline__ bool eval_staged(const GraphView &g, const WarpSmem &s, RowStage &st,
+                                            const uint32_t *cid, uint32_t *ckey, int nc, int srows,
+                                            bool first_issued, int lane) {
+  if (nc > srows) prefetch_rows(g, cid + srows, nc - srows, lane);
+  const int h = lane & 1, c = lane >> 1;
+  for (int p0 = 0; p0 < nc; p0 += srows) {
+    const int m = min(srows, nc - p0);
+    if (p0 > 0 || !first_issued) stage_issue(g, s, st, cid + p0, m, lane);
+    if (!stage_wait(st)) return false;
+    const float d = staged_distance<NB>(g, s.q, s.stage + (c < m ? c : 0) * (g.nb * 8), h);
+    if (h == 0 && c < m) ckey[p0 + c] = float_to_key(d);
+    __syncwarp();
   }
+  return true;
 }
 
 // Loads this lane's share of a node's adjacency row.
@@ -496,25 +599,57 @@ __device__ __forceinline__ void prefetch_adj_l2(const GraphView &g, uint32_t nod
                : "memory");
 }
 
+// Rank of each accepted candidate among the accepted ones by (key, adjacency
+// position): lane-held candidate i = t*32 + lane.  The pool position of
+// candidate i after the merge is its rank plus its pool rank acle[i].
+template <int RCH>
+__device__ __forceinline__ void accepted_positions(const WarpSmem &s, int na, int lane,
+                                                   uint32_t (&nkey)[RCH], uint32_t (&nid)[RCH],
+                                                   int (&npos)[RCH], int L) {
+  int rank[RCH];
+#pragma unroll
+  for (int t = 0; t < RCH; ++t) {
+    const int i = t * 32 + lane;
+    nkey[t] = i < na ? s.ak[i] : 0xFFFFFFFFu;
+    nid[t] = i < na ? s.aid[i] : 0u;
+    rank[t] = 0;
+  }
+#pragma unroll 4
+  for (int j = 0; j < na; ++j) {
+    const uint32_t kj = s.ak[j];
+#pragma unroll
+    for (int t = 0; t < RCH; ++t) {
+      const int i = t * 32 + lane;
+      rank[t] += (kj < nkey[t]) || (kj == nkey[t] && j < i);
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < RCH; ++t) {
+    const int i = t * 32 + lane;
+    npos[t] = i < na ? rank[t] + (int)s.acle[i] : L;
+  }
+}
+
 // One query, one warp.  Each hop (batch-merge form of annsearch.cpp:218-253):
-//   1. expand the first unexplored pool slot k (all slots before `cursor` are
-//      explored); u is the unexplored slot after it;
+//   1. expand pool slot k, the first unexplored one (known from the previous
+//      hop); u is the unexplored slot after it;
 //   2. read k's adjacency row; drop ids already visited and mark the rest
 //      visited, the first occurrence in adjacency order winning (:229-231);
-//   3. compute their distances (:236);
+//   3. compute their distances (:236) from rows staged in shared memory;
 //   4. accept d < pool[size-1] taken at the start of the hop (:238); each
-//      accepted key's rank in the pool (entries <= key) is its merge offset;
-//   5. sort accepted candidates by (d, adjacency position) and stable-merge
-//      them into the pool, older entries first on ties, truncated to L
-//      (InsertIntoPool upper-bound insert, util.h:56-75; :242-243).
-// The next expansion is known after step 4 (u, unless the best accepted
-// candidate lands before it), so its adjacency row is loaded while step 5
-// runs; u's row is also sent to L2 at the start of the hop.
+//      accepted key's rank in the pool (entries <= key) plus its rank among
+//      the accepted ones by (d, adjacency position) is its new slot;
+//   5. stable-merge the accepted candidates into the pool, older entries
+//      first on ties, truncated to L (InsertIntoPool upper-bound insert,
+//      util.h:56-75; :242-243).
+// After step 4 the next expansion is known (u, unless the best accepted
+// candidate lands before it), so its adjacency row loads during step 5, and
+// u's row is sent to L2 at the start of the hop.
 template <int NB, int RCH>
 __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qsrc, int K, int L,
                                 uint32_t *out_ids, float *out_dists, uint32_t *out_ndc,
                                 uint32_t *out_hops, int32_t *out_status, const WarpSmem &s,
-                                const SmemPlan &p, uint32_t max_hops, int lane) {
+                                const SmemPlan &p, RowStage &st, uint32_t max_hops, int lane) {
   const unsigned lanemask_lt = (1u << lane) - 1u;
   const int qw = (int)g.nb * 8;
   for (int i = lane; i < qw; i += 32) s.q[i] = i < (int)g.dim ? qsrc[i] : 0.f;
@@ -546,14 +681,40 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
       const unsigned peers = __match_any_sync(kFull, row[c]);
       const bool leader = valid && (peers & lanemask_lt) == 0u;
       if (valid) s.cid[m] = row[c];
-      qh_visit_warp(vis, row[c], leader);
+      QProbe pr{};
+      const bool found = leader && qh_lookup(vis, row[c], pr);
+      qh_record(vis, pr, row[c], leader && !found, lane);
+      __syncwarp();
       size += __popc(__ballot_sync(kFull, valid));
     }
     __syncwarp();
-    eval_all<NB>(g, s.q, s.cid, s.ckey, size, lane);
+    if (!eval_staged<NB>(g, s, st, s.cid, s.ckey, size, (int)p.stage_rows, false, lane)) {
+      status = kStatusStageTimeout;
+      size = 0;
+    }
     ndc += size;
+    // pool = candidates ranked by (key, position): every candidate counts as
+    // accepted with pool rank 0
+#pragma unroll
+    for (int c = 0; c < RCH; ++c) {
+      const int e = c * 32 + lane;
+      if (e < size) {
+        s.ak[e] = s.ckey[e];
+        s.aid[e] = s.cid[e];
+        s.acle[e] = 0u;
+      }
+    }
     __syncwarp();
-    rank_sort<RCH>(s.ckey, s.cid, s.cid, size, s.pk, s.pid, s.sid, lane);
+    uint32_t nkey[RCH], nid[RCH];
+    int npos[RCH];
+    accepted_positions<RCH>(s, size, lane, nkey, nid, npos, L);
+#pragma unroll
+    for (int c = 0; c < RCH; ++c) {
+      if (npos[c] < L) {
+        s.pk[npos[c]] = nkey[c];
+        s.pid[npos[c]] = nid[c];
+      }
+    }
     __syncwarp();
   }
 
@@ -564,31 +725,26 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
     load_row<RCH>(g, pref_node, lane, pref_row);
   }
 
-  int cursor = 0;
-  for (;;) {
-    // 1. first two unexplored slots at or after the cursor
-    int k = -1, u = -1;
-    for (int b0 = cursor; b0 < size; b0 += 32) {
+  int k = size > 0 ? 0 : -1;  // first unexplored slot
+  while (k >= 0) {
+    if (hops >= max_hops) {
+      status = kStatusHopLimit;
+      break;
+    }
+    // 1. u: the first unexplored slot after k
+    int u = -1;
+    for (int b0 = k + 1; b0 < size; b0 += 32) {
       const int idx = b0 + lane;
       const bool un = idx < size && !(s.pid[idx] & kExplored);
-      unsigned bm = __ballot_sync(kFull, un);
-      if (k < 0 && bm) {
-        k = b0 + __ffs(bm) - 1;
-        bm &= bm - 1u;
-      }
+      const unsigned bm = __ballot_sync(kFull, un);
       if (bm) {
         u = b0 + __ffs(bm) - 1;
         break;
       }
     }
-    if (k < 0) break;
-    if (hops >= max_hops) {
-      status = kStatusHopLimit;
-      break;
-    }
     const uint32_t node = s.pid[k];
     const uint32_t thr = s.pk[size - 1];
-    const uint32_t unode = u >= 0 ? (s.pid[u] & ~kExplored) : kNoneId;
+    const uint32_t unode = u >= 0 ? s.pid[u] : kNoneId;
     __syncwarp();
     if (lane == 0) {
       s.pid[k] = node | kExplored;
@@ -603,30 +759,44 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
       load_row<RCH>(g, node, lane, row);
     }
 
-    // 2. in-row dedupe, visited filter, compaction in m order
+    // 2. in-row dedupe, visited filter, compaction in m order.  The row
+    //    copies of the first stage load start as soon as the fresh ids are
+    //    known; the table is updated while they are in flight.
     int nc = 0;
+    const int srows = (int)p.stage_rows;
+    bool issued = false;
 #pragma unroll
     for (int c = 0; c < RCH; ++c) {
       const bool valid = row[c] != kNoneId;
       const unsigned peers = __match_any_sync(kFull, row[c]);
       const bool leader = valid && (peers & lanemask_lt) == 0u;
-      const bool fresh = qh_visit_warp(vis, row[c], leader);
+      QProbe pr{};
+      const bool fresh = leader && !qh_lookup(vis, row[c], pr);
       const unsigned fm = __ballot_sync(kFull, fresh);
       if (fresh) s.cid[nc + __popc(fm & lanemask_lt)] = row[c];
       nc += __popc(fm);
+      if (RCH == 1 && nc > 0) {
+        __syncwarp();
+        stage_issue(g, s, st, s.cid, min(nc, srows), lane);
+        issued = true;
+      }
+      qh_record(vis, pr, row[c], fresh, lane);
+      __syncwarp();
     }
     if (nc == 0) {
       pref_node = unode;
       if (unode != kNoneId) load_row<RCH>(g, unode, lane, pref_row);
-      cursor = k + 1;
+      k = u;
       continue;
     }
     __syncwarp();
 
-    // 3. distances (rows prefetched to L2 together, then 16 per pass)
-    eval_all<NB>(g, s.q, s.cid, s.ckey, nc, lane);
+    // 3. distances of the staged rows
+    if (!eval_staged<NB>(g, s, st, s.cid, s.ckey, nc, srows, issued, lane)) {
+      status = kStatusStageTimeout;
+      break;
+    }
     ndc += nc;
-    __syncwarp();
 
     // 4. acceptance in adjacency order, with each key's pool rank; after an
     //    eviction, a candidate already in the pool (same id under the same
@@ -664,57 +834,37 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
     if (na == 0) {
       pref_node = unode;
       if (unode != kNoneId) load_row<RCH>(g, unode, lane, pref_row);
-      cursor = k + 1;
+      k = u;
       continue;
     }
     __syncwarp();
-
-    // Next expansion: the best accepted candidate (smallest key, then first
-    // in adjacency order) lands at p0 = its pool rank; old slot u stays ahead
-    // of it iff u < p0.  Its adjacency row loads during the sort and merge.
-    int p0;
-    {
-      uint32_t bk = 0xFFFFFFFFu;
-      int be = 0x7FFFFFFF;
-#pragma unroll
-      for (int c = 0; c < RCH; ++c) {
-        const int e = c * 32 + lane;
-        if (e < na) {
-          const uint32_t kk = s.ak[e];
-          if (kk < bk) {
-            bk = kk;
-            be = e;
-          }
-        }
-      }
-      const uint32_t kmin = __reduce_min_sync(kFull, bk);
-      const int emin = (int)__reduce_min_sync(kFull, bk == kmin ? (uint32_t)be : 0x7FFFFFFFu);
-      p0 = (int)s.acle[emin];
-      const uint32_t nxt = (u >= 0 && u < p0) ? unode : s.aid[emin];
-      pref_node = nxt;
-      load_row<RCH>(g, nxt, lane, pref_row);
-    }
-
-    rank_sort<RCH>(s.ak, s.aid, s.acle, na, s.sk, s.sid, s.scle, lane);
-    __syncwarp();
-
-    // 5. stable merge into the pool, in place.  New entry e (sorted rank)
-    //    goes to e + its pool rank; old entries at and after p0 move up by
-    //    the number of new keys below them, in 128-entry windows from the top
-    //    down, 4 entries per lane, each window fully read before it is
-    //    written.
     uint32_t nkey[RCH], nid[RCH];
     int npos[RCH];
+    accepted_positions<RCH>(s, na, lane, nkey, nid, npos, L);
+
+    // Next expansion: the best accepted candidate lands at p0 (the smallest
+    // new slot); old slot u stays ahead of it iff u < p0.  Its adjacency row
+    // loads during the merge.
+    int pmin = npos[0];
 #pragma unroll
-    for (int c = 0; c < RCH; ++c) {
-      const int e = c * 32 + lane;
-      npos[c] = L;
-      if (e < na) {
-        nkey[c] = s.sk[e];
-        nid[c] = s.sid[e];
-        npos[c] = e + (int)s.scle[e];
-      }
+    for (int c = 1; c < RCH; ++c) pmin = min(pmin, npos[c]);
+    const int p0 = (int)__reduce_min_sync(kFull, (uint32_t)pmin);
+    {
+      uint32_t cand = kNoneId;
+#pragma unroll
+      for (int c = 0; c < RCH; ++c)
+        if (npos[c] == p0) cand = nid[c];
+      const uint32_t best = __reduce_min_sync(kFull, cand);  // the one lane holding p0
+      const uint32_t nxt = (u >= 0 && u < p0) ? unode : best;
+      pref_node = nxt;
+      load_row<RCH>(g, nxt, lane, pref_row);
+      k = (u >= 0 && u < p0) ? u : p0;
     }
+
+    // 5. stable merge into the pool, in place: old entries at and after p0
+    //    move up by the number of new keys below them, in 128-entry windows
+    //    from the top down, 4 entries per lane, each window fully read before
+    //    it is written; then the new entries go to their slots.
     for (int w = ((size - 1) >> 7) << 7; w + 128 > p0 && w >= 0; w -= 128) {
       const int j0 = w + 4 * lane;
       const bool any = j0 + 3 >= p0 && j0 < size;
@@ -724,8 +874,9 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
         ii = *reinterpret_cast<const uint4 *>(s.pid + j0);
       }
       int c0 = 0, c1 = 0, c2 = 0, c3 = 0;
+#pragma unroll 4
       for (int i = 0; i < na; ++i) {
-        const uint32_t sv = s.sk[i];
+        const uint32_t sv = s.ak[i];
         c0 += kk.x > sv;
         c1 += kk.y > sv;
         c2 += kk.z > sv;
@@ -750,15 +901,13 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
     }
 #pragma unroll
     for (int c = 0; c < RCH; ++c) {
-      const int e = c * 32 + lane;
-      if (e < na && npos[c] < L) {
+      if (npos[c] < L) {
         s.pk[npos[c]] = nkey[c];
         s.pid[npos[c]] = nid[c];
       }
     }
     __syncwarp();
     size = min(L, size + na);
-    cursor = min(k + 1, p0);
   }
 
   // Results: slots the pool never filled keep the reference's value-
@@ -776,14 +925,22 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
   __syncwarp();
 }
 
-// At most 128 registers a thread (two 256-thread CTAs' worth per SM): whole
-// rows stay in flight per lane pair and up to 16 query teams fit an SM.
+// At most 128 registers a thread (two 256-thread CTAs' worth per SM).
 template <int NB, int RCH>
 __global__ void __launch_bounds__(256, 2) warp_search_kernel(GraphView g, BatchArgs a, SmemPlan p) {
-  extern __shared__ __align__(16) uint32_t smem[];
+  extern __shared__ __align__(128) uint32_t smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wpb = blockDim.x >> 5;
   const WarpSmem s = carve_warp(smem + (size_t)warp * p.words_per_team, p);
+  RowStage st;
+  st.bar = smem_addr(s.bar);
+  st.phase = 0;
+  st.broken = false;
+  if (lane == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(st.bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
   const uint32_t slot = blockIdx.x * wpb + warp;
   const uint32_t nslots = gridDim.x * wpb;
   uint32_t q = slot;
@@ -803,7 +960,13 @@ __global__ void __launch_bounds__(256, 2) warp_search_kernel(GraphView g, BatchA
       warp_search_one<NB, RCH>(g, a.queries + (size_t)q * a.qstride, K, L, a.ids + off,
                                a.dists ? a.dists + off : nullptr, a.ndc ? a.ndc + q : nullptr,
                                a.hops ? a.hops + q : nullptr, a.status ? a.status + q : nullptr, s,
-                               p, a.max_hops, lane);
+                               p, st, a.max_hops, lane);
+      // a stage copy that never completed leaves this team's stage unusable:
+      // wait once more (bounded) for it and take no further queries
+      if (st.broken) {
+        mbar_wait(st.bar, st.phase ^ 1u);
+        break;
+      }
     }
     if (!a.work_counter) q += nslots;
   }
@@ -856,7 +1019,7 @@ __device__ __forceinline__ uint32_t st_find_or_insert(uint32_t *tab, uint32_t ma
 template <int NB, int RCH>
 __global__ void __launch_bounds__(512) intra_search_kernel(GraphView g, BatchArgs a, SmemPlan p,
                                                            int W) {
-  extern __shared__ __align__(16) uint32_t smem[];
+  extern __shared__ __align__(128) uint32_t smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nthr = blockDim.x;
   const unsigned lanemask_lt = (1u << lane) - 1u;
@@ -1235,9 +1398,13 @@ SmemPlan plan_warp_smem(const GraphView &g, int L_max, int hash_cap_override) {
   p.q_words = g.nb * 8;
   p.pool_cap = round_up((uint32_t)L_max, 32);
   p.cand_cap = round_up(g.rstride, 32);
-  // visited table: buckets of 8 tags; default about 20 slots per unit of L
+  // Visited table: buckets of 8 tags.  It may forget (see QHash), so its
+  // size trades shared memory (teams resident per SM) against repeated
+  // distance evaluations; the default, 2 slots per unit of L and at least
+  // 1024, measured fastest on the 1.2M x 200 workload at L = 200 and 400.
   uint32_t slots = hash_cap_override > 0 ? pow2_at_least((uint32_t)hash_cap_override)
-                                         : pow2_at_least((uint32_t)L_max * 20u);
+                                         : pow2_at_least((uint32_t)L_max * 2u);
+  if (slots < 1024 && hash_cap_override <= 0) slots = 1024;
   if (slots < 512) slots = 512;
   if (slots > 65536) slots = 65536;
   uint32_t bbits = log2_of(slots / 8);
@@ -1249,8 +1416,13 @@ SmemPlan plan_warp_smem(const GraphView &g, int L_max, int hash_cap_override) {
   p.qh_rbits = nbits > bbits ? nbits - bbits : 0;
   p.hash_cap = (1u << bbits) * 8;
   p.hash_limit = p.hash_cap;
-  p.words_per_team = p.q_words + 2 * p.pool_cap + 8 * p.cand_cap + (1u << bbits) * 4;
-  p.words_per_team = round_up(p.words_per_team, 4);
+  // row stage: 16 rows, fewer for rows so wide that 16 would pass 64 KB
+  p.stage_rows = kStageRows;
+  while (p.stage_rows > 1 && p.stage_rows * g.nb * 32u > 65536u) p.stage_rows >>= 1;
+  p.stage_words = p.stage_rows * g.nb * 8;
+  p.words_per_team = p.stage_words + 4 + p.q_words + 2 * p.pool_cap + 5 * p.cand_cap +
+                     (1u << bbits) * 4;
+  p.words_per_team = round_up(p.words_per_team, 32);  // 128-byte aligned stages
   return p;
 }
 

@@ -233,6 +233,15 @@ def test_device_api_matches_host_api(oracle_lib):
     assert _same_bits(d.cpu().numpy(), d_h)
     _, _, o_ndc, o_hops = oracle_lib.search(fx["base"], fx["adj"], int(fx["ep"]), 1, fx["queries"],
                                             20, 64)
+    # the traversal is the reference's hop for hop; a visited table that
+    # forgot ids only adds distance evaluations
+    assert np.array_equal(hops.cpu().numpy().view(np.uint32), o_hops)
+    assert (ndc.cpu().numpy().view(np.uint32) >= o_ndc).all()
+    # with a table large enough never to forget, the counts are the reference's
+    idx.set_tuning(hash_cap=65536)
+    idx.search_batch_device(q, nq, ids, d, K=20, L=64, ndc=ndc, hops=hops, stream=s.cuda_stream)
+    s.synchronize()
+    assert np.array_equal(ids.cpu().numpy().view(np.uint32), ids_h)
     assert np.array_equal(ndc.cpu().numpy().view(np.uint32), o_ndc)
     assert np.array_equal(hops.cpu().numpy().view(np.uint32), o_hops)
     idx.close()
