@@ -143,6 +143,28 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
+PROFILED_TRAFFIC = {
+    # (workload, L, queries) -> ncu summary holding the DRAM bytes of one launch
+    ("cfg3", 400, 10000): "profiles/warp_search_kernel_1.2Mx200_ip_L400.md",
+}
+
+
+def profiled_traffic(workload, L, nq):
+    """DRAM bytes (read + write) of one search launch from the committed ncu
+    summary of this exact workload, or None when none was captured."""
+    rel = PROFILED_TRAFFIC.get((workload, L, nq))
+    if not rel:
+        return None, None
+    try:
+        with open(os.path.join(ROOT, rel)) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1]), rel
+    except OSError:
+        pass
+    return None, None
+
+
 def measured_hbm_peak():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -428,6 +450,7 @@ def run_ours(args):
     plain_same = bool(np.array_equal(plain_ids, ids_np[:ns]))
 
     peak, peak_kind = measured_hbm_peak()
+    traffic, traffic_src = profiled_traffic(args.workload, L, nq)
     mean_step_s = sum(step_ms) / len(step_ms) / 1000.0
     achieved = bytes_per_step / mean_step_s / 1e9
 
@@ -449,7 +472,8 @@ def run_ours(args):
                       "ids_equal_batched": plain_same,
                       "batched_over_plain": qps / d.world / plain_qps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                     "traffic_source": traffic_src,
                      "algorithmic_bytes_per_query": bytes_per_step / nq,
                      "ndc_per_query": float(ndc.mean()), "hops_per_query": float(hops.mean()),
                      "distance_evals_per_s": float(ndc.sum()) / mean_step_s,

@@ -123,6 +123,27 @@ class ANNSearch {
                  handle, "SearchBatch");
   }
 
+  // Batched extension with per-query K and L; query i's results start at
+  // Ks[0] + ... + Ks[i-1] of ids.
+  void SearchBatchUneven(const float *queries, unsigned nq, const std::vector<int32_t> &Ks,
+                         const std::vector<int32_t> &Ls, std::vector<unsigned> &ids,
+                         std::vector<float> *dists = nullptr) {
+    size_t total = 0;
+    for (unsigned i = 0; i < nq; ++i) total += (size_t)Ks[i];
+    ids.resize(total);
+    if (dists) dists->resize(total);
+    die_on_error(ss_search_batch_uneven(handle, queries, nq, Ks.data(), Ls.data(),
+                                        reinterpret_cast<uint32_t *>(ids.data()),
+                                        dists ? dists->data() : nullptr),
+                 handle, "SearchBatchUneven");
+  }
+
+  // Launch tuning of the batched kernel (ss_set_tuning; 0 = automatic).
+  void SetTuning(int warps_per_block = 0, int hash_cap = 0, int blocks_per_sm_cap = 0) {
+    die_on_error(ss_set_tuning(handle, warps_per_block, hash_cap, blocks_per_sm_cap), handle,
+                 "SetTuning");
+  }
+
   std::vector<uint32_t> graph_table(unsigned rstride) const {
     std::vector<uint32_t> out((size_t)base_num * rstride);
     die_on_error(ss_get_graph(handle, out.data(), rstride), handle, "graph_table");
