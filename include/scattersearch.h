@@ -49,7 +49,9 @@ enum ss_status {
   SS_ERR_CUDA = 5,             /* CUDA runtime error (message has details)    */
   SS_ERR_OUT_OF_MEMORY = 6,    /* device or host allocation failed            */
   SS_ERR_UNSUPPORTED = 7,      /* parameter outside the compiled limits       */
-  SS_ERR_SEARCH_LIMIT = 8      /* a query hit the device hop limit            */
+  SS_ERR_SEARCH_LIMIT = 8,     /* a query hit the device hop limit            */
+  SS_ERR_BUSY = 9,             /* the server's request queue is full          */
+  SS_ERR_TIMEOUT = 10          /* a wait for a request ran out of time        */
 };
 
 /* Largest beam width (pool size L) and graph degree the kernels accept. */
@@ -204,6 +206,67 @@ int ss_search_intra_batch_device(ss_index *h, const float *queries, uint32_t nq,
  * but never changes results);
  * blocks_per_sm_cap: limit on resident CTAs per SM (0 = occupancy limit). */
 int ss_set_tuning(ss_index *h, int warps_per_block, int hash_cap, int blocks_per_sm_cap);
+
+/* ---- serving ------------------------------------------------------------ */
+
+/* Online search service over one index.  Replaces the reference's online
+ * driver (tests/online_parallel_search.cpp:91-160: a generator thread pushes
+ * queries into a mutex-guarded deque, one consumer searches them one at a
+ * time).  Here requests arrive one at a time (ss_server_submit) and are
+ * batched continuously: a dispatcher thread launches everything pending (up
+ * to max_batch requests, each with its own K and L) as soon as one of its
+ * launch slots is free, so requests that arrive while others run on the GPU
+ * are admitted as slots free up and their launches overlap on the device.
+ * The number of slots is bounded by free device memory at creation.  Index,
+ * queries, pools and visited tables stay on the device; each result is
+ * exactly the ss_search result for that query, whatever it was batched
+ * with. */
+typedef struct ss_server ss_server;
+
+typedef struct ss_server_config {
+  uint32_t max_batch;     /* most requests per launch (1..4096); 0 = 256               */
+  uint32_t max_inflight;  /* most launches on the GPU at once (1..16); 0 = 4           */
+  uint32_t max_pending;   /* queued requests before submit says SS_ERR_BUSY; 0 = 1<<16 */
+  int32_t K_max;          /* largest K a request may ask for; 0 = 100                   */
+  int32_t L_max;          /* largest L a request may ask for; 0 = 512                   */
+  float memory_fraction;  /* share of free device memory the slots may take; 0 = 0.25  */
+} ss_server_config;
+
+typedef struct ss_server_stats {
+  uint64_t submitted, completed, failed, batches;
+  double mean_batch;                  /* requests per launch                      */
+  double p50_us, p99_us, p999_us;     /* arrival-to-result latency, completed ones */
+  double max_us;
+  uint32_t slots;                     /* launch slots the memory budget allowed   */
+} ss_server_stats;
+
+/* Starts the dispatcher.  cfg may be NULL (all defaults).  The index must
+ * have a graph and outlive the server. */
+int ss_server_create(ss_index *h, const ss_server_config *cfg, ss_server **out);
+
+/* Queues one request (query: dim floats on the host, copied).  Returns
+ * SS_ERR_BUSY when max_pending requests are already queued. */
+int ss_server_submit(ss_server *s, const float *query, int K, int L, uint64_t *ticket);
+
+/* Waits up to timeout_ms (< 0: no limit) for a request, copies its K ids and
+ * distances (dists may be NULL) and its latency in microseconds (may be
+ * NULL), and forgets the ticket. */
+int ss_server_wait(ss_server *s, uint64_t ticket, int timeout_ms, uint32_t *ids, float *dists,
+                   double *latency_us);
+
+/* Load replay: submits request i at arrival_us[i] microseconds after the call
+ * starts (a generator thread; arrival_us ascending), waits for all, and
+ * writes results at offset Ks[0] + ... + Ks[i-1] of ids/dists and each
+ * latency (from its arrival time) to latency_us[i]. */
+int ss_server_replay(ss_server *s, const float *queries, uint32_t nq, const int32_t *Ks,
+                     const int32_t *Ls, const double *arrival_us, uint32_t *ids, float *dists,
+                     double *latency_us);
+
+/* Counters and latency percentiles since creation (or the last reset). */
+int ss_server_get_stats(ss_server *s, ss_server_stats *out, int reset);
+
+/* Finishes the launches in flight, drops queued requests, frees the slots. */
+void ss_server_destroy(ss_server *s);
 
 /* ---- host I/O (util.cpp) ---------------------------------------------- */
 

@@ -15,7 +15,7 @@ SS_OK = 0
 STATUS_NAMES = {
     0: "SS_OK", 1: "SS_ERR_INVALID_ARGUMENT", 2: "SS_ERR_IO", 3: "SS_ERR_FORMAT",
     4: "SS_ERR_NO_GRAPH", 5: "SS_ERR_CUDA", 6: "SS_ERR_OUT_OF_MEMORY", 7: "SS_ERR_UNSUPPORTED",
-    8: "SS_ERR_SEARCH_LIMIT",
+    8: "SS_ERR_SEARCH_LIMIT", 9: "SS_ERR_BUSY", 10: "SS_ERR_TIMEOUT",
 }
 SS_MAX_L = 4096
 SS_MAX_DEGREE = 128
@@ -53,12 +53,38 @@ SIGNATURES = {
     "ss_search_intra_batch_device": (_i32, [_vp, _vp, _u32, _i32, _i32, _i32, _vp, _vp, _vp, _vp,
                                             _vp]),
     "ss_set_tuning": (_i32, [_vp, _i32, _i32, _i32]),
+    "ss_server_create": (_i32, [_vp, _vp, _hp]),
+    "ss_server_submit": (_i32, [_vp, _f32p, _i32, _i32, ctypes.POINTER(ctypes.c_uint64)]),
+    "ss_server_wait": (_i32, [_vp, ctypes.c_uint64, _i32, _u32p, _f32p,
+                              ctypes.POINTER(ctypes.c_double)]),
+    "ss_server_replay": (_i32, [_vp, _f32p, _u32, _i32p, _i32p, ctypes.POINTER(ctypes.c_double),
+                                _u32p, _f32p, ctypes.POINTER(ctypes.c_double)]),
+    "ss_server_get_stats": (_i32, [_vp, _vp, _i32]),
+    "ss_server_destroy": (None, [_vp]),
     "ss_load_fbin": (_i32, [ctypes.c_char_p, ctypes.POINTER(_f32p), _u32p, _u32p]),
     "ss_load_groundtruth": (_i32, [ctypes.c_char_p, ctypes.POINTER(_u32p), _u32p, _u32p]),
     "ss_free": (None, [_vp]),
     "ss_last_error": (ctypes.c_char_p, [_vp]),
     "ss_version": (ctypes.c_char_p, []),
 }
+
+
+
+class ServerConfig(ctypes.Structure):
+    """ss_server_config (include/scattersearch.h)."""
+    _fields_ = [("max_batch", ctypes.c_uint32), ("max_inflight", ctypes.c_uint32),
+                ("max_pending", ctypes.c_uint32), ("K_max", ctypes.c_int32),
+                ("L_max", ctypes.c_int32), ("memory_fraction", ctypes.c_float)]
+
+
+class ServerStats(ctypes.Structure):
+    """ss_server_stats (include/scattersearch.h)."""
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64),
+                ("failed", ctypes.c_uint64), ("batches", ctypes.c_uint64),
+                ("mean_batch", ctypes.c_double), ("p50_us", ctypes.c_double),
+                ("p99_us", ctypes.c_double), ("p999_us", ctypes.c_double),
+                ("max_us", ctypes.c_double), ("slots", ctypes.c_uint32)]
+
 
 _lib = None
 

@@ -376,6 +376,47 @@ int create_common(uint32_t dim, uint32_t num, const float *src, bool src_on_devi
 
 }  // namespace
 
+// Host-side hooks for the serving loop (ss_server.cpp), declared in
+// ss_internal.h.
+namespace ssb {
+
+int index_device(const ss_index *h) { return h->device; }
+uint32_t index_dim(const ss_index *h) { return h->dim; }
+bool index_ready(const ss_index *h) { return h && h->has_graph; }
+
+int index_error(ss_index *h, int code, const char *msg) { return set_err(h, code, "%s", msg); }
+
+int server_launch(ss_index *h, const float *d_q, uint32_t nq, const int32_t *d_K,
+                  const int32_t *d_L, const int64_t *d_off, int L_max, uint32_t *d_ids,
+                  float *d_dists, int32_t *d_status, uint32_t *d_counter, cudaStream_t stream) {
+  ssb::GraphView g = h->view();
+  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, h->hash_cap_override);
+  const int wpb = choose_wpb(h, plan);
+  if ((size_t)plan.words_per_team * 4 * wpb > 227 * 1024)
+    return set_err(h, SS_ERR_UNSUPPORTED, "L=%d needs %u bytes of shared memory per query",
+                   L_max, plan.words_per_team * 4);
+  const int blocks = persistent_blocks(h, plan, wpb, nq);
+  if (blocks <= 0) return set_err(h, SS_ERR_UNSUPPORTED, "search kernel cannot be resident");
+  ssb::BatchArgs a{};
+  a.queries = d_q;
+  a.qstride = h->dim;
+  a.nq = nq;
+  a.Ks = d_K;
+  a.Ls = d_L;
+  a.out_off = d_off;
+  a.ids = d_ids;
+  a.dists = d_dists;
+  a.status = d_status;
+  a.work_counter = d_counter;
+  a.max_hops = h->n + 1;
+  SS_CUDA(h, cudaMemsetAsync(d_counter, 0, 4, stream), "counter reset");
+  SS_CUDA(h, cudaMemsetAsync(d_status, 0, (size_t)nq * 4, stream), "status reset");
+  SS_CUDA(h, ssb::launch_warp_search(g, a, plan, wpb, blocks, stream), "search launch");
+  return SS_OK;
+}
+
+}  // namespace ssb
+
 extern "C" {
 
 const char *ss_version(void) { return "scattersearch_b200 0.1 sm_100a"; }

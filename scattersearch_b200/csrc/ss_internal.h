@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+struct ss_index;
+
 namespace ssb {
 
 constexpr uint32_t kNoneId = 0xFFFFFFFFu;
@@ -96,5 +98,20 @@ cudaError_t noalloc_scratch(NoallocScratch *out);
 // Adds the number of nonzero status[0..nq) to *failed.
 cudaError_t launch_count_failed(const int32_t *status, uint32_t nq, uint32_t *failed,
                                 cudaStream_t stream);
+
+// ---- host-side hooks of the C ABI layer (ss_api.cpp) used by the serving
+// loop (ss_server.cpp).  `ss_index` is the opaque handle of
+// include/scattersearch.h.
+int index_device(const ::ss_index *h);
+uint32_t index_dim(const ::ss_index *h);
+bool index_ready(const ::ss_index *h);
+// Records `msg` as the handle's last error and returns `code`.
+int index_error(::ss_index *h, int code, const char *msg);
+// Enqueues one batched search of nq device-resident queries with per-query K
+// and L (device arrays) on `stream`; results of query i start at d_off[i].
+// d_status (nq words) and d_counter (1 word) are scratch owned by the caller.
+int server_launch(::ss_index *h, const float *d_q, uint32_t nq, const int32_t *d_K,
+                  const int32_t *d_L, const int64_t *d_off, int L_max, uint32_t *d_ids,
+                  float *d_dists, int32_t *d_status, uint32_t *d_counter, cudaStream_t stream);
 
 }  // namespace ssb
