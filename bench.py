@@ -64,6 +64,8 @@ def parse_args(argv=None):
     ap.add_argument("--plain-sample", type=int, default=300)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-online", action="store_true",
+                    help="skip the serving and intra-query latency legs")
     return ap.parse_args(argv)
 
 
@@ -333,6 +335,73 @@ def pick_L(idx, wl, target=0.95):
     return res[-1][0], res[-1][1], res
 
 
+def measure_online(idx, wl, L, rates=(100_000, 300_000, 550_000), seconds=0.15):
+    """Serving leg: Poisson arrivals replayed through the continuous-batching
+    server (ss_server_replay); latency is arrival to result on the host."""
+    from scattersearch_b200.serving import Server, poisson_arrivals
+    K = wl["K"]
+    Q = wl["queries"]
+    out = []
+    with Server(idx, max_batch=512, max_inflight=4, K_max=K, L_max=L) as srv:
+        warm = min(len(Q), 4096)
+        srv.replay(Q[:warm], np.full(warm, K, np.int32), np.full(warm, L, np.int32),
+                   poisson_arrivals(warm, 100_000, seed=1))
+        srv.stats(reset=True)
+        for rate in rates:
+            n = int(max(2000, rate * seconds))
+            q = Q[np.arange(n) % len(Q)]
+            t0 = time.perf_counter()
+            _, _, _, lat = srv.replay(q, np.full(n, K, np.int32), np.full(n, L, np.int32),
+                                      poisson_arrivals(n, rate, seed=rate))
+            wall = time.perf_counter() - t0
+            st = srv.stats(reset=True)
+            out.append({"offered_qps": rate, "requests": n, "sustained_qps": n / wall,
+                        "p50_ms": float(np.percentile(lat, 50)) / 1e3,
+                        "p99_ms": float(np.percentile(lat, 99)) / 1e3,
+                        "p999_ms": float(np.percentile(lat, 99.9)) / 1e3,
+                        "mean_batch": st["mean_batch"]})
+            log(f"online {rate}/s: p50 {out[-1]['p50_ms']:.2f} ms p99 {out[-1]['p99_ms']:.2f} ms")
+    return {"K": K, "L": L, "max_batch": 512, "slots": 4, "arrivals": "Poisson",
+            "latency": "arrival to result on the host", "rates": out}
+
+
+def measure_intra_latency(idx, wl, L, device, batches=(1, 4, 16), widths=(4, 8), reps=10):
+    """Device time of one small batch: the plain kernel (one warp per query)
+    and the intra-query kernel (one CTA of W warps per query, W candidates
+    expanded per step), with recall@10 of each."""
+    import torch
+    K = wl["K"]
+    Q = wl["Q"]
+    st = torch.cuda.current_stream()
+    res = []
+    for b in batches:
+        ids = torch.empty((b, K), dtype=torch.int32, device=device)
+        row = {"batch": b}
+        for W in (0,) + tuple(widths):
+            ms, hits = [], []
+            for r in range(reps):
+                q = Q[r * b:(r + 1) * b]
+                run = (lambda: idx.search_batch_device(q, b, ids, None, K=K, L=L,
+                                                       stream=st.cuda_stream)) if W == 0 else \
+                      (lambda: idx.search_intra_batch_device(q, b, K, L, W, ids,
+                                                             stream=st.cuda_stream))
+                run()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                run()
+                e1.record(st)
+                torch.cuda.synchronize()
+                ms.append(e0.elapsed_time(e1))
+                hits.append(recall_at_10(ids.cpu().numpy().view(np.uint32),
+                                         wl["gt"][r * b:(r + 1) * b]))
+            key = "plain" if W == 0 else f"intra_w{W}"
+            row[key] = {"ms": float(np.median(ms)), "recall@10": float(np.mean(hits))}
+        res.append(row)
+        log(f"batch {b}: " + ", ".join(f"{k} {v['ms']:.2f} ms" for k, v in row.items()
+                                          if k != "batch"))
+    return {"K": K, "L": L, "timing": "CUDA events, median of %d batches" % reps, "rows": res}
+
+
 def run_ours(args):
     import torch
     d = Dist("nccl")
@@ -366,9 +435,11 @@ def run_ours(args):
     stream = torch.cuda.current_stream()
 
     def step(with_stats=False):
-        idx.search_batch_device(Qd, nq, ids_d, dist_d, K=K, L=L,
-                                ndc=ndc_d if with_stats else None,
-                                hops=hops_d if with_stats else None, stream=stream.cuda_stream)
+        if with_stats:
+            idx.search_batch_device(Qd, nq, ids_d, dist_d, K=K, L=L, ndc=ndc_d, hops=hops_d,
+                                    stream=stream.cuda_stream)
+        else:  # the launch captured in a CUDA graph, replayed
+            plan.launch(stream.cuda_stream)
 
     # Stats passes (same traversal, same ids).  The algorithmic bytes count
     # the reference algorithm's distance evaluations, taken with a visited
@@ -388,6 +459,7 @@ def run_ours(args):
     ndc_dev = ndc_d.cpu().numpy().astype(np.int64)
     if not np.array_equal(ids_d.cpu().numpy(), ids_exact):
         raise RuntimeError("ids depend on the visited-table size")
+    plan = idx.plan_batch_device(Qd, nq, K, L, ids_d, dist_d)
     rstride = idx.rstride
     bytes_per_step = float(ndc.sum() * 4 * dim + hops.sum() * 4 * rstride + nq * 4 * dim)
     row_bytes = 4 * ((dim + 7) // 8 * 8)
@@ -413,6 +485,8 @@ def run_ours(args):
     d.barrier()
     clocks = sampler.stop()
     step_ms = [s.elapsed_time(e) for s, e in evs]
+    if plan.failed_queries():
+        raise RuntimeError("graph-captured search reported failed queries")
     total_s = d.max(sum(step_ms) / 1000.0, device)
     qps = nq * d.world * args.steps / total_s
     ids_np = ids_d.cpu().numpy().view(np.uint32)
@@ -449,6 +523,9 @@ def run_ours(args):
     plain_qps = ns / plain_s
     plain_same = bool(np.array_equal(plain_ids, ids_np[:ns]))
 
+    online = None if args.no_online else measure_online(idx, wl, L)
+    intra = None if args.no_online else measure_intra_latency(idx, wl, L, device)
+
     peak, peak_kind = measured_hbm_peak()
     traffic, traffic_src = profiled_traffic(args.workload, L, nq)
     mean_step_s = sum(step_ms) / len(step_ms) / 1000.0
@@ -479,7 +556,10 @@ def run_ours(args):
                      "distance_evals_per_s": float(ndc.sum()) / mean_step_s,
                      "device_evals_per_query": float(ndc_dev.mean()),
                      "device_row_gbps": device_bytes_per_step / mean_step_s / 1e9},
+        "online": online,
+        "intra_latency": intra,
         "gpu_launches": args.steps,
+        "launch": "one CUDA graph per step (queue reset, status reset, search kernel)",
         "clocks": clocks,
     }
     if d.rank == 0 and d.world == 1 and not args.no_cpu_baseline:
@@ -495,6 +575,7 @@ def run_ours(args):
                 "ids_equal_gpu_fraction": float((cids == ids_np[:sample]).all(1).mean())}
         else:
             out["cpu_baseline"] = None
+    plan.close()
     idx.close()
     if d.rank == 0:
         print(json.dumps(out))

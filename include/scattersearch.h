@@ -143,6 +143,22 @@ int ss_search_batch_device(ss_index *h, const float *queries, uint32_t nq, const
                            uint32_t *ids, float *dists, uint32_t *ndc, uint32_t *hops,
                            void *stream);
 
+/* Graph-captured batched search.  No counterpart in the reference.
+ * ss_plan_create records one ss_search_batch_device launch (uniform K and
+ * L; queries, ids and dists are fixed device buffers; dists may be NULL) --
+ * the work-queue reset, the status reset and the persistent search kernel --
+ * into a CUDA graph; ss_plan_launch replays it on `stream` with one graph
+ * launch.  The plan owns its status words: ss_plan_status reports the failed
+ * queries of its last synchronised replay.  Buffers must stay valid while
+ * the plan exists; rewrite the query buffer between replays to search new
+ * queries. */
+typedef struct ss_plan ss_plan;
+int ss_plan_create(ss_index *h, const float *queries, uint32_t nq, int K, int L, uint32_t *ids,
+                   float *dists, ss_plan **out);
+int ss_plan_launch(ss_plan *p, void *stream);
+int ss_plan_status(ss_plan *p, uint32_t *failed_queries);
+void ss_plan_destroy(ss_plan *p);
+
 /* After a synchronised ss_search_batch_device: number of queries of the last
  * device batch on this handle whose status was nonzero. */
 int ss_batch_status(ss_index *h, uint32_t *failed_queries);

@@ -47,6 +47,10 @@ SIGNATURES = {
     "ss_search_batch_device": (_i32, [_vp, _vp, _u32, _vp, _vp, _vp, _i32, _i32, _i32, _vp, _vp,
                                       _vp, _vp, _vp]),
     "ss_batch_status": (_i32, [_vp, _u32p]),
+    "ss_plan_create": (_i32, [_vp, _vp, _u32, _i32, _i32, _vp, _vp, _hp]),
+    "ss_plan_launch": (_i32, [_vp, _vp]),
+    "ss_plan_status": (_i32, [_vp, _u32p]),
+    "ss_plan_destroy": (None, [_vp]),
     "ss_search_batch_noalloc": (_i32, [_vp, _vp, _u32, _i32, _i32, _vp, _vp, _vp]),
     "ss_search_intra": (_i32, [_vp, _f32p, _i32, _i32, _i32, _u32p, _f32p]),
     "ss_search_intra_batch": (_i32, [_vp, _f32p, _u32, _i32, _i32, _i32, _u32p, _f32p]),

@@ -261,6 +261,14 @@ class ANNSearch:
             self._h, _dptr(queries), int(nq), int(K), int(L), _dptr(ids), _dptr(dists),
             ctypes.c_void_p(int(stream)) if stream else None))
 
+    def plan_batch_device(self, queries, nq: int, K: int, L: int, ids, dists=None):
+        """Captures the batched device search on these fixed buffers into a
+        CUDA graph (ss_plan_create); returns a ``SearchPlan``."""
+        p = ctypes.c_void_p()
+        self._check(self._lib.ss_plan_create(self._h, _dptr(queries), int(nq), int(K), int(L),
+                                             _dptr(ids), _dptr(dists), ctypes.byref(p)))
+        return SearchPlan(self, p)
+
     def batch_status(self) -> int:
         """Failed queries of the last device batch (call after synchronising)."""
         n = ctypes.c_uint32()
@@ -270,3 +278,33 @@ class ANNSearch:
     def set_tuning(self, warps_per_block: int = 0, hash_cap: int = 0, blocks_per_sm_cap: int = 0):
         self._check(self._lib.ss_set_tuning(self._h, int(warps_per_block), int(hash_cap),
                                             int(blocks_per_sm_cap)))
+
+
+class SearchPlan:
+    """A graph-captured batched search (ss_plan_*): ``launch(stream)``
+    replays the recorded launch with one CUDA graph launch."""
+
+    def __init__(self, index, handle):
+        self._index = index
+        self._lib = index._lib
+        self._p = handle
+
+    def launch(self, stream=None):
+        self._index._check(self._lib.ss_plan_launch(
+            self._p, ctypes.c_void_p(int(stream)) if stream else None))
+
+    def failed_queries(self) -> int:
+        n = ctypes.c_uint32()
+        self._index._check(self._lib.ss_plan_status(self._p, ctypes.byref(n)))
+        return n.value
+
+    def close(self):
+        if self._p:
+            self._lib.ss_plan_destroy(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # pragma: no cover - interpreter shutdown
+            pass

@@ -680,6 +680,119 @@ int ss_search_batch_device(ss_index *h, const float *queries, uint32_t nq, const
                       hops, static_cast<cudaStream_t>(stream), true);
 }
 
+}  // extern "C"
+
+struct ss_plan {
+  ss_index *h = nullptr;
+  uint32_t nq = 0;
+  int32_t *status = nullptr;
+  uint32_t *counter = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+void plan_free(ss_plan *p) {
+  if (!p) return;
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  if (p->status) cudaFree(p->status);
+  if (p->counter) cudaFree(p->counter);
+  delete p;
+}
+}  // namespace
+
+extern "C" {
+
+int ss_plan_create(ss_index *h, const float *queries, uint32_t nq, int K, int L, uint32_t *ids,
+                   float *dists, ss_plan **out) {
+  if (!out) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null output plan");
+  *out = nullptr;
+  int rc = check_search_args(h, K, L);
+  if (rc) return rc;
+  if (nq == 0 || !queries || !ids)
+    return set_err(h, SS_ERR_INVALID_ARGUMENT, "a plan needs nq > 0, queries and ids");
+  DeviceGuard dg(h->device);
+  auto *p = new ss_plan();
+  p->h = h;
+  p->nq = nq;
+  cudaStream_t cs = nullptr;
+  cudaError_t e = cudaMalloc(&p->status, (size_t)nq * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&p->counter, 16);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    plan_free(p);
+    if (cs) cudaStreamDestroy(cs);
+    std::lock_guard<std::mutex> lk(h->mu);
+    return cuda_fail(h, e, "plan allocation");
+  }
+  // Plan the launch outside the capture (occupancy queries and kernel
+  // attributes are not stream work).
+  ssb::GraphView g = h->view();
+  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L, h->hash_cap_override);
+  const int wpb = choose_wpb(h, plan);
+  const int blocks = persistent_blocks(h, plan, wpb, nq);
+  if ((size_t)plan.words_per_team * 4 * wpb > 227 * 1024 || blocks <= 0) {
+    plan_free(p);
+    cudaStreamDestroy(cs);
+    return set_err(h, SS_ERR_UNSUPPORTED, "L=%d cannot be planned on this device", L);
+  }
+  ssb::BatchArgs a{};
+  a.queries = queries;
+  a.qstride = h->dim;
+  a.nq = nq;
+  a.K0 = K;
+  a.L0 = L;
+  a.ids = ids;
+  a.dists = dists;
+  a.status = p->status;
+  a.work_counter = p->counter;
+  a.max_hops = h->n + 1;
+  e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    cudaError_t e1 = cudaMemsetAsync(p->counter, 0, 4, cs);
+    cudaError_t e2 = cudaMemsetAsync(p->status, 0, (size_t)nq * 4, cs);
+    cudaError_t e3 = ssb::launch_warp_search(g, a, plan, wpb, blocks, cs);
+    e = cudaStreamEndCapture(cs, &p->graph);
+    if (e == cudaSuccess) e = e1 != cudaSuccess ? e1 : e2 != cudaSuccess ? e2 : e3;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec, p->graph, 0);
+  cudaStreamDestroy(cs);
+  if (e != cudaSuccess) {
+    plan_free(p);
+    std::lock_guard<std::mutex> lk(h->mu);
+    return cuda_fail(h, e, "graph capture of the search launch");
+  }
+  *out = p;
+  return SS_OK;
+}
+
+int ss_plan_launch(ss_plan *p, void *stream) {
+  if (!p) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null plan");
+  DeviceGuard dg(p->h->device);
+  SS_CUDA(p->h, cudaGraphLaunch(p->exec, static_cast<cudaStream_t>(stream)), "graph launch");
+  return SS_OK;
+}
+
+int ss_plan_status(ss_plan *p, uint32_t *failed_queries) {
+  if (!p || !failed_queries) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null argument");
+  DeviceGuard dg(p->h->device);
+  std::vector<int32_t> st(p->nq);
+  SS_CUDA(p->h, cudaMemcpy(st.data(), p->status, (size_t)p->nq * 4, cudaMemcpyDeviceToHost),
+          "status download");
+  uint32_t bad = 0;
+  for (int32_t v : st) bad += v != 0;
+  *failed_queries = bad;
+  return SS_OK;
+}
+
+void ss_plan_destroy(ss_plan *p) {
+  if (!p) return;
+  DeviceGuard dg(p->h->device);
+  cudaDeviceSynchronize();
+  plan_free(p);
+}
+
 int ss_batch_status(ss_index *h, uint32_t *failed_queries) {
   if (!h || !failed_queries) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null argument");
   DeviceGuard dg(h->device);

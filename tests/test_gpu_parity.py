@@ -291,3 +291,27 @@ def test_reference_style_driver_surface(oracle_lib):
     out2 = idx.MultiThreadSearchArraySimulationWithET(fx["queries"][0], 0, 10, 50, 1, flags, tmp)
     assert np.array_equal(out, out2)
     idx.close()
+
+
+def test_graph_captured_plan_matches_direct_launch(oracle_lib):
+    import torch
+    fx = load_fixture("search_l2_d200")
+    idx = _index(fx["base"], fx["adj"], fx["ep"], 0)
+    Q = fx["queries"]
+    half = len(Q) // 2
+    q = torch.as_tensor(Q[:half]).cuda()
+    ids = torch.empty((half, 10), dtype=torch.int32, device="cuda")
+    d = torch.empty((half, 10), dtype=torch.float32, device="cuda")
+    plan = idx.plan_batch_device(q, half, 10, 100, ids, d)
+    s = torch.cuda.current_stream()
+    for part in (Q[:half], Q[half:2 * half], Q[:half]):  # new queries in the same buffer
+        q.copy_(torch.as_tensor(part))
+        plan.launch(s.cuda_stream)
+        s.synchronize()
+        assert plan.failed_queries() == 0
+        o_ids, o_d, _, _ = oracle_lib.search(fx["base"], fx["adj"], int(fx["ep"]), 0, part, 10,
+                                             100)
+        assert np.array_equal(ids.cpu().numpy().view(np.uint32), o_ids)
+        assert _same_bits(d.cpu().numpy(), o_d)
+    plan.close()
+    idx.close()
