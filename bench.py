@@ -29,6 +29,7 @@ time is the maximum over ranks.
 from __future__ import annotations
 
 import argparse
+import contextlib
 import datetime
 import json
 import os
@@ -49,6 +50,25 @@ FALLBACK_HBM_GBS = 6650.0
 
 def log(*a):
     print("[bench]", *a, file=sys.stderr, flush=True)
+
+
+@contextlib.contextmanager
+def stdout_to_stderr():
+    """Sends file descriptor 1 to stderr for the duration (the reference
+    library prints to stdout; the bench's stdout carries one JSON line)."""
+    import ctypes
+    sys.stdout.flush()
+    libc = ctypes.CDLL(None)
+    libc.fflush(None)
+    saved = os.dup(1)
+    os.dup2(2, 1)
+    try:
+        yield
+    finally:
+        libc.fflush(None)
+        sys.stdout.flush()
+        os.dup2(saved, 1)
+        os.close(saved)
 
 
 def parse_args(argv=None):
@@ -224,6 +244,11 @@ def cpu_threads():
 
 
 def time_reference(wl, L, seconds, fast=True, warm=1):
+    with stdout_to_stderr():
+        return _time_reference(wl, L, seconds, fast, warm)
+
+
+def _time_reference(wl, L, seconds, fast=True, warm=1):
     """Reference SearchArraySimulation on the host cores over a bounded
     sample; returns (qps, sample size, ids of the sample, threads)."""
     from oracle import oracle as O
@@ -248,16 +273,23 @@ def time_reference(wl, L, seconds, fast=True, warm=1):
 
 
 def run_reference_arm(args):
+    with stdout_to_stderr():
+        out = _reference_arm(args)
+    if out is not None:
+        print(json.dumps(out))
+    return 0
+
+
+def _reference_arm(args):
     d = Dist("gloo")
     if d.rank != 0:
         d.close()
-        return 0
+        return None
     import torch
     from oracle import oracle as O
     if not O.have_reference(fast=True):
-        print(json.dumps({"impl": "reference",
-                          "unavailable": "oracle/_ref/libssref_fast.so was not built"}))
-        return 0
+        d.close()
+        return {"impl": "reference", "unavailable": "oracle/_ref/libssref_fast.so was not built"}
     device = torch.device("cuda", d.local_rank) if torch.cuda.is_available() else "cpu"
     wl = build_workload(args, 0, 1, device)
     L = choose_L_reference(args, wl)
@@ -299,8 +331,8 @@ def run_reference_arm(args):
         "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(out))
-    return 0
+    d.close()
+    return out
 
 
 def choose_L_reference(args, wl):
@@ -374,6 +406,7 @@ def measure_intra_latency(idx, wl, L, device, batches=(1, 4, 16), widths=(4, 8),
     Q = wl["Q"]
     st = torch.cuda.current_stream()
     res = []
+    idx.set_tuning()  # the tuned table size is the batched kernel's; use automatic sizes here
     for b in batches:
         ids = torch.empty((b, K), dtype=torch.int32, device=device)
         row = {"batch": b}
@@ -427,6 +460,11 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         L = int(t.item())
 
+    # launch layout (teams per CTA, visited-table size) tuned on a sample
+    from scattersearch_b200 import autotune
+    tune = autotune.autotune(idx, wl["Q"], K, L, reps=2, path=None)
+    log(f"tuned: {tune['warps_per_block']} teams per CTA, {tune['hash_cap']}-slot visited table")
+
     Qd = wl["Q"]
     ids_d = torch.empty((nq, K), dtype=torch.int32, device=device)
     dist_d = torch.empty((nq, K), dtype=torch.float32, device=device)
@@ -453,7 +491,7 @@ def run_ours(args):
     ndc = ndc_d.cpu().numpy().astype(np.int64)
     hops = hops_d.cpu().numpy().astype(np.int64)
     ids_exact = ids_d.cpu().numpy().copy()
-    idx.set_tuning()
+    idx.set_tuning(tune["warps_per_block"], tune["hash_cap"], 0)
     step(with_stats=True)
     torch.cuda.synchronize()
     ndc_dev = ndc_d.cpu().numpy().astype(np.int64)
@@ -525,6 +563,7 @@ def run_ours(args):
 
     online = None if args.no_online else measure_online(idx, wl, L)
     intra = None if args.no_online else measure_intra_latency(idx, wl, L, device)
+    idx.set_tuning(tune["warps_per_block"], tune["hash_cap"], 0)
 
     peak, peak_kind = measured_hbm_peak()
     traffic, traffic_src = profiled_traffic(args.workload, L, nq)
@@ -542,7 +581,10 @@ def run_ours(args):
                    "mean_degree": float((wl["adj"] != 0xFFFFFFFF).sum(1).mean()),
                    "l2": "inputs larger than L2 (base %.0f MB > 126 MB L2)"
                          % (wl["X"].numel() * 4 / 1e6),
-                   "parallelism": f"replicas x{d.world}, queries sharded"},
+                   "parallelism": f"replicas x{d.world}, queries sharded",
+                   "tuning": {"warps_per_block": tune["warps_per_block"],
+                              "hash_cap": tune["hash_cap"],
+                              "sample": f"the {nq} bench queries (launch layout only)"}},
         "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": nq * dim * 4,
                 "d2h_bytes_per_step": nq * K * 8, "ids_equal_device_path": same_ids},
         "plain_gpu": {"value": plain_qps, "unit": "queries/s", "sample": ns,

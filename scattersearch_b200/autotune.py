@@ -1,0 +1,129 @@
+"""Launch autotuner of the batched search kernel.
+
+The reference has no tunables beyond compile-time macros.  Here the batched
+warp-per-query kernel exposes two layout choices that change speed but never
+results: how many query teams share a CTA (``warps_per_block``) and the size
+of each query's shared-memory visited table (``hash_cap``; a smaller table
+fits more teams per SM but forgets more visited ids, which are then evaluated
+again).  ``autotune`` times candidate pairs on a sample of the caller's
+queries with CUDA events, checks that every candidate returns the same ids,
+and keeps the fastest.  Choices are cached per (GPU name, dim, adjacency row
+stride, L rounded up to a power of two) in a JSON file, so ``apply`` can
+reuse them without timing.
+"""
+from __future__ import annotations
+
+import json
+import os
+import threading
+
+import numpy as np
+
+DEFAULT_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "scattersearch_b200",
+                             "tuning.json")
+WPB_CANDIDATES = (1, 2, 4, 8)
+_lock = threading.Lock()
+
+
+def l_bucket(L: int) -> int:
+    """L rounded up to a power of two (tuning keys cover L ranges)."""
+    b = 1
+    while b < L:
+        b <<= 1
+    return b
+
+
+def hash_candidates(L: int):
+    """Visited-table sizes worth timing for beam width L."""
+    lo = 1024
+    hi = max(lo, min(65536, l_bucket(L) * 32))
+    out, c = [], lo
+    while c <= hi:
+        out.append(c)
+        c <<= 1
+    return out
+
+
+def tuning_key(gpu: str, dim: int, rstride: int, L: int) -> str:
+    return f"{gpu}|dim={dim}|rstride={rstride}|L<={l_bucket(L)}"
+
+
+def load_cache(path: str = DEFAULT_CACHE) -> dict:
+    try:
+        with open(path) as f:
+            data = json.load(f)
+        return data if isinstance(data, dict) else {}
+    except (OSError, ValueError):
+        return {}
+
+
+def save_choice(key: str, choice: dict, path: str = DEFAULT_CACHE) -> None:
+    with _lock:
+        data = load_cache(path)
+        data[key] = choice
+        os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
+        tmp = path + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(data, f, indent=1, sort_keys=True)
+        os.replace(tmp, path)
+
+
+def _gpu_name(device) -> str:
+    import torch
+    return torch.cuda.get_device_name(device)
+
+
+def apply(index, L: int, path: str = DEFAULT_CACHE, device=None) -> dict | None:
+    """Sets the cached choice for (this GPU, index shape, L) on ``index``;
+    returns it, or None (and leaves the automatic setting) when none is
+    cached."""
+    key = tuning_key(_gpu_name(device), index.dimension, index.rstride, L)
+    choice = load_cache(path).get(key)
+    if choice:
+        index.set_tuning(int(choice["warps_per_block"]), int(choice["hash_cap"]), 0)
+    return choice
+
+
+def autotune(index, queries, K: int, L: int, reps: int = 3, path: str | None = DEFAULT_CACHE,
+             device=None, wpb_candidates=WPB_CANDIDATES, hash_caps=None) -> dict:
+    """Times every (warps_per_block, hash_cap) candidate on ``queries`` (a
+    CUDA tensor, nq x dim) and sets the fastest on ``index``.  Raises if two
+    candidates return different ids.  Returns the choice with the timing
+    table; stores it in the cache at ``path`` (None: no cache)."""
+    import torch
+    nq = int(queries.shape[0])
+    dev = queries.device
+    ids = torch.empty((nq, K), dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    ref = None
+    table = []
+    for hc in (hash_caps or hash_candidates(L)):
+        for wpb in wpb_candidates:
+            index.set_tuning(wpb, hc, 0)
+            index.search_batch_device(queries, nq, ids, None, K=K, L=L,
+                                      stream=stream.cuda_stream)
+            stream.synchronize()
+            got = ids.cpu().numpy()
+            if ref is None:
+                ref = got.copy()
+            elif not np.array_equal(got, ref):
+                raise RuntimeError(f"ids differ under warps_per_block={wpb}, hash_cap={hc}")
+            times = []
+            for _ in range(reps):
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                index.search_batch_device(queries, nq, ids, None, K=K, L=L,
+                                          stream=stream.cuda_stream)
+                b.record(stream)
+                stream.synchronize()
+                times.append(a.elapsed_time(b))
+            table.append({"warps_per_block": wpb, "hash_cap": hc, "ms": float(np.median(times))})
+    best = min(table, key=lambda r: r["ms"])
+    index.set_tuning(best["warps_per_block"], best["hash_cap"], 0)
+    choice = {"warps_per_block": best["warps_per_block"], "hash_cap": best["hash_cap"],
+              "ms": best["ms"], "sample_queries": nq, "K": K, "L": L}
+    if path:
+        save_choice(tuning_key(_gpu_name(device if device is not None else dev),
+                               index.dimension, index.rstride, L), choice, path)
+    return dict(choice, table=table)

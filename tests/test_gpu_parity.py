@@ -315,3 +315,21 @@ def test_graph_captured_plan_matches_direct_launch(oracle_lib):
         assert _same_bits(d.cpu().numpy(), o_d)
     plan.close()
     idx.close()
+
+
+def test_autotuner_keeps_results_and_caches_its_choice(oracle_lib, tmp_path):
+    import torch
+    from scattersearch_b200 import autotune
+    fx = load_fixture("search_ip_d96")
+    idx = _index(fx["base"], fx["adj"], fx["ep"], 1)
+    q = torch.as_tensor(fx["queries"]).cuda()
+    before, _ = idx.search_batch(fx["queries"], 10, 100)
+    path = str(tmp_path / "tuning.json")
+    choice = autotune.autotune(idx, q, 10, 100, reps=1, path=path)
+    assert choice["warps_per_block"] in (1, 2, 4, 8) and choice["hash_cap"] >= 1024
+    assert len(choice["table"]) == 4 * len(autotune.hash_candidates(100))
+    after, _ = idx.search_batch(fx["queries"], 10, 100)
+    assert np.array_equal(before, after)
+    idx.set_tuning()
+    assert autotune.apply(idx, 100, path=path)["hash_cap"] == choice["hash_cap"]
+    idx.close()

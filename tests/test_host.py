@@ -155,3 +155,20 @@ def test_replica_sharding_over_gloo(tmp_path, oracle_lib):
     one, *_ = oracle_lib.search(fx["base"], fx["adj"], int(fx["ep"]), 0, fx["queries"], 10, 50)
     assert np.array_equal(np.load(tmp_path / "ids.npy"), one)
     assert float(np.load(tmp_path / "t.npy")[0]) == 2.0
+
+
+def test_autotune_keys_and_cache(tmp_path):
+    from scattersearch_b200 import autotune as at
+    assert [at.l_bucket(x) for x in (1, 64, 65, 400)] == [1, 64, 128, 512]
+    hc = at.hash_candidates(400)
+    assert hc[0] == 1024 and hc[-1] == 16384 and all(b == 2 * a for a, b in zip(hc, hc[1:]))
+    assert at.hash_candidates(16) == [1024]
+    k1 = at.tuning_key("NVIDIA B200", 200, 32, 400)
+    assert k1 == at.tuning_key("NVIDIA B200", 200, 32, 300)  # same L bucket
+    assert k1 != at.tuning_key("NVIDIA B200", 200, 32, 600)
+    path = str(tmp_path / "t" / "tuning.json")
+    assert at.load_cache(path) == {}
+    at.save_choice(k1, {"warps_per_block": 2, "hash_cap": 2048}, path)
+    at.save_choice("other", {"warps_per_block": 1, "hash_cap": 1024}, path)
+    data = at.load_cache(path)
+    assert data[k1]["hash_cap"] == 2048 and set(data) == {k1, "other"}
