@@ -223,6 +223,25 @@ int ss_search_intra_batch_device(ss_index *h, const float *queries, uint32_t nq,
  * blocks_per_sm_cap: limit on resident CTAs per SM (0 = occupancy limit). */
 int ss_set_tuning(ss_index *h, int warps_per_block, int hash_cap, int blocks_per_sm_cap);
 
+/* ---- exact brute force -------------------------------------------------- */
+
+/* Exact k nearest base rows of each query by brute force (no graph needed);
+ * replaces the reference's external ground-truth files (load_groundtruth,
+ * src/util.cpp:72-93) and gives the graph builder exact k-NN lists.
+ * Inner products run on the tensor cores (TF32 in three terms, FP32
+ * accumulation) to select candidates; the candidates are then re-ranked with
+ * the search's exact distance (the reference's FP32 lane model), so ids and
+ * distances are those of an exact scan, ties broken by smaller id.
+ * ids/dists: nq x k (dists may be NULL); rows beyond the index size get id
+ * 0xFFFFFFFF.  1 <= k <= 112. */
+int ss_bruteforce(ss_index *h, const float *queries, uint32_t nq, int k, uint32_t *ids,
+                  float *dists);
+
+/* Device-pointer form (queries nq x dim on the device), asynchronous on
+ * `stream`. */
+int ss_bruteforce_device(ss_index *h, const float *queries, uint32_t nq, int k, uint32_t *ids,
+                         float *dists, void *stream);
+
 /* ---- serving ------------------------------------------------------------ */
 
 /* Online search service over one index.  Replaces the reference's online

@@ -57,6 +57,8 @@ SIGNATURES = {
     "ss_search_intra_batch_device": (_i32, [_vp, _vp, _u32, _i32, _i32, _i32, _vp, _vp, _vp, _vp,
                                             _vp]),
     "ss_set_tuning": (_i32, [_vp, _i32, _i32, _i32]),
+    "ss_bruteforce": (_i32, [_vp, _f32p, _u32, _i32, _u32p, _f32p]),
+    "ss_bruteforce_device": (_i32, [_vp, _vp, _u32, _i32, _vp, _vp, _vp]),
     "ss_server_create": (_i32, [_vp, _vp, _hp]),
     "ss_server_submit": (_i32, [_vp, _f32p, _i32, _i32, ctypes.POINTER(ctypes.c_uint64)]),
     "ss_server_wait": (_i32, [_vp, ctypes.c_uint64, _i32, _u32p, _f32p,

@@ -212,6 +212,22 @@ class ANNSearch:
                                                      _ptr(dists, _f32p)))
         return ids, dists
 
+    def bruteforce(self, queries, k: int):
+        """Exact k nearest base rows of each query (tensor-core candidate scan,
+        exact re-rank; ties by id).  Returns (ids, dists), nq x k."""
+        q = _f32(queries).reshape(-1, self.dimension)
+        nq = q.shape[0]
+        ids = np.empty((nq, k), dtype=np.uint32)
+        dists = np.empty((nq, k), dtype=np.float32)
+        self._check(self._lib.ss_bruteforce(self._h, _ptr(q, _f32p), nq, int(k), _ptr(ids, _u32p),
+                                            _ptr(dists, _f32p)))
+        return ids, dists
+
+    def bruteforce_device(self, queries, nq: int, k: int, ids, dists=None, stream=None):
+        self._check(self._lib.ss_bruteforce_device(
+            self._h, _dptr(queries), int(nq), int(k), _dptr(ids), _dptr(dists),
+            ctypes.c_void_p(int(stream)) if stream else None))
+
     def search_intra(self, query, K: int, L: int, num_threads: int):
         q = _f32(query).reshape(-1)
         ids = np.empty(K, dtype=np.uint32)

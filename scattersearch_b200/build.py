@@ -23,7 +23,7 @@ INCLUDE = os.path.join(ROOT, "include")
 OBJDIR = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libscattersearch_b200.so")
 
-SOURCES = ["ss_search.cu", "ss_api.cpp", "ss_server.cpp"]
+SOURCES = ["ss_search.cu", "ss_bruteforce.cu", "ss_api.cpp", "ss_server.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-O3",
                      "-I" + INCLUDE, "-I" + CSRC]

@@ -71,7 +71,7 @@ struct DevBuf {
 // Per-caller launch state: one stream plus the buffers a search needs.
 struct SearchCtx {
   cudaStream_t stream = nullptr;
-  DevBuf q, ids, dists, Ks, Ls, off, counter, status, ndc, hops, spill;
+  DevBuf q, ids, dists, Ks, Ls, off, counter, status, ndc, hops, spill, bf_q, bf_cand;
   std::vector<int32_t> h_status;
   ~SearchCtx() {
     if (stream) cudaStreamDestroy(stream);
@@ -100,6 +100,11 @@ struct ss_index {
   std::mutex dev_mu;  // device-batch scratch
   SearchCtx dev_ctx;
   uint32_t dev_last_nq = 0;
+
+  // squared row norms for the L2 brute force, computed on first use
+  std::mutex norm_mu;
+  DevBuf xnorm;
+  bool have_norms = false;
 
   // launch tuning (set by the autotuner through ss_set_tuning); 0 = automatic
   int warps_per_block = 0;
@@ -791,6 +796,104 @@ void ss_plan_destroy(ss_plan *p) {
   DeviceGuard dg(p->h->device);
   cudaDeviceSynchronize();
   plan_free(p);
+}
+
+}  // extern "C"
+
+namespace {
+// Brute force of nq device queries (row stride `qstride` floats) into device
+// ids/dists on `stream`, with scratch from `c`.
+int bruteforce_common(ss_index *h, SearchCtx *c, const float *d_queries, size_t qstride,
+                      uint32_t nq, int k, uint32_t *d_ids, float *d_dists, cudaStream_t stream) {
+  const uint32_t pitch = h->nb * 8;
+  const float *xnorm = nullptr;
+  if (h->metric == SS_METRIC_L2) {
+    std::lock_guard<std::mutex> lk(h->norm_mu);
+    if (!h->have_norms) {
+      SS_CUDA(h, h->xnorm.ensure((size_t)h->n * 4), "norm buffer");
+      SS_CUDA(h, ssb::launch_norms(h->base.as<float>(), h->n, pitch, h->xnorm.as<float>(), stream),
+              "norm launch");
+      h->have_norms = true;
+    }
+    xnorm = h->xnorm.as<float>();
+  }
+  ssb::BrutePlan bp = ssb::plan_bruteforce(h->n, nq, k, h->sm_count);
+  SS_CUDA(h, c->bf_q.ensure((size_t)nq * pitch * 4), "query buffer");
+  SS_CUDA(h, c->bf_cand.ensure((size_t)nq * bp.splits * bp.C * 8), "candidate buffer");
+  SS_CUDA(h, cudaMemsetAsync(c->bf_q.p, 0, (size_t)nq * pitch * 4, stream), "query clear");
+  SS_CUDA(h, cudaMemcpy2DAsync(c->bf_q.p, (size_t)pitch * 4, d_queries, qstride * 4,
+                               (size_t)h->dim * 4, nq, cudaMemcpyDeviceToDevice, stream),
+          "query copy");
+  ssb::BruteArgs a{};
+  a.base = h->base.as<float>();
+  a.n = h->n;
+  a.nb = h->nb;
+  a.queries = c->bf_q.as<float>();
+  a.nq = nq;
+  a.xnorm = xnorm;
+  a.metric = h->metric;
+  a.k = k;
+  a.C = bp.C;
+  a.splits = bp.splits;
+  a.rows_per_split = bp.rows_per_split;
+  a.cand = c->bf_cand.as<uint64_t>();
+  a.ids = d_ids;
+  a.dists = d_dists;
+  SS_CUDA(h, ssb::launch_bruteforce(a, h->view(), stream), "brute-force launch");
+  return SS_OK;
+}
+
+int check_bruteforce_args(ss_index *h, int k) {
+  if (!h) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null index handle");
+  if (k < 1) return set_err(h, SS_ERR_INVALID_ARGUMENT, "need k >= 1 (got %d)", k);
+  if (k > ssb::kBruteMaxK)
+    return set_err(h, SS_ERR_UNSUPPORTED, "k=%d exceeds the brute force's limit of %d", k,
+                   ssb::kBruteMaxK);
+  return SS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int ss_bruteforce(ss_index *h, const float *queries, uint32_t nq, int k, uint32_t *ids,
+                  float *dists) {
+  int rc = check_bruteforce_args(h, k);
+  if (rc) return rc;
+  if (nq == 0) return SS_OK;
+  if (!queries || !ids) return set_err(h, SS_ERR_INVALID_ARGUMENT, "null queries or ids");
+  DeviceGuard dg(h->device);
+  CtxLease lease(h);
+  SearchCtx *c = lease.c;
+  if (!c) return set_err(h, SS_ERR_CUDA, "cannot create a stream");
+  const size_t total = (size_t)nq * k;
+  SS_CUDA(h, c->q.ensure((size_t)nq * h->dim * 4), "query buffer");
+  SS_CUDA(h, c->ids.ensure(total * 4), "ids buffer");
+  SS_CUDA(h, c->dists.ensure(total * 4), "dists buffer");
+  SS_CUDA(h, cudaMemcpyAsync(c->q.p, queries, (size_t)nq * h->dim * 4, cudaMemcpyHostToDevice,
+                             c->stream),
+          "query upload");
+  rc = bruteforce_common(h, c, c->q.as<float>(), h->dim, nq, k, c->ids.as<uint32_t>(),
+                         c->dists.as<float>(), c->stream);
+  if (rc) return rc;
+  SS_CUDA(h, cudaMemcpyAsync(ids, c->ids.p, total * 4, cudaMemcpyDeviceToHost, c->stream),
+          "ids download");
+  if (dists)
+    SS_CUDA(h, cudaMemcpyAsync(dists, c->dists.p, total * 4, cudaMemcpyDeviceToHost, c->stream),
+            "dists download");
+  SS_CUDA(h, cudaStreamSynchronize(c->stream), "brute force");
+  return SS_OK;
+}
+
+int ss_bruteforce_device(ss_index *h, const float *queries, uint32_t nq, int k, uint32_t *ids,
+                         float *dists, void *stream) {
+  int rc = check_bruteforce_args(h, k);
+  if (rc) return rc;
+  if (nq == 0) return SS_OK;
+  if (!queries || !ids) return set_err(h, SS_ERR_INVALID_ARGUMENT, "null queries or ids");
+  DeviceGuard dg(h->device);
+  std::lock_guard<std::mutex> lk(h->dev_mu);
+  return bruteforce_common(h, &h->dev_ctx, queries, h->dim, nq, k, ids, dists,
+                           static_cast<cudaStream_t>(stream));
 }
 
 int ss_batch_status(ss_index *h, uint32_t *failed_queries) {

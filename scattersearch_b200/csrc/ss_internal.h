@@ -99,6 +99,31 @@ cudaError_t noalloc_scratch(NoallocScratch *out);
 cudaError_t launch_count_failed(const int32_t *status, uint32_t nq, uint32_t *failed,
                                 cudaStream_t stream);
 
+// ---- brute-force k-NN (ss_bruteforce.cu) --------------------------------
+struct BruteArgs {
+  const float *base;      // n x (nb*8), padded rows
+  uint32_t n, nb;
+  const float *queries;   // nq x (nb*8), padded with zeros
+  uint32_t nq;
+  const float *xnorm;     // n squared norms (L2 only)
+  int metric;
+  int k, C;               // results per query; candidates kept per split (32/64/128)
+  uint32_t splits, rows_per_split;
+  uint64_t *cand;         // nq x splits x C scratch
+  uint32_t *ids;          // nq x k
+  float *dists;           // nq x k, may be null
+};
+struct BrutePlan {
+  int C;
+  uint32_t splits, rows_per_split;
+};
+// Largest k the brute force accepts (candidates kept = k + 16 <= 128).
+constexpr int kBruteMaxK = 112;
+BrutePlan plan_bruteforce(uint32_t n, uint32_t nq, int k, int sm_count);
+cudaError_t launch_norms(const float *base, uint32_t n, uint32_t pitch, float *out,
+                         cudaStream_t s);
+cudaError_t launch_bruteforce(const BruteArgs &a, const GraphView &g, cudaStream_t s);
+
 // ---- host-side hooks of the C ABI layer (ss_api.cpp) used by the serving
 // loop (ss_server.cpp).  `ss_index` is the opaque handle of
 // include/scattersearch.h.
