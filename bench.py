@@ -219,14 +219,43 @@ def build_workload(args, rank, world, device):
     adj, ep = graph.build_graph(X, R=w.graph_R, knn_k=w.graph_knn, device=device)
     log(f"graph R={w.graph_R} ep={ep} mean degree {(adj != 0xFFFFFFFF).sum(1).mean():.1f} "
         f"in {time.time() - t0:.1f}s")
-    t0 = time.time()
     Q = torch.from_numpy(queries).to(device)
-    gt, _ = graph.bruteforce(X, Q, 10, w.metric)
-    log(f"ground truth in {time.time() - t0:.1f}s")
     if device != "cpu" and torch.cuda.is_available():
         torch.cuda.empty_cache()  # hand the graph build's scratch back to the driver
+    gt, gt_info = ground_truth(X, Q, w.metric, device)
+    log(f"ground truth: {gt_info}")
     return dict(spec=spec, w=w, X=X, queries=queries, Q=Q, adj=adj, ep=ep,
-                gt=gt.cpu().numpy(), metric=w.metric, K=spec["K"])
+                gt=gt, gt_info=gt_info, metric=w.metric, K=spec["K"])
+
+
+def ground_truth(X, Q, metric, device, k=10):
+    """Exact top-10 of every query: the library's tensor-core brute force
+    (timed with CUDA events), or torch when the library is not built."""
+    import torch
+    nq, dim = Q.shape
+    n = X.shape[0]
+    try:
+        from scattersearch_b200 import ANNSearch
+        idx = ANNSearch(dim, n, X, metric, base_on_device=True)
+    except Exception as e:  # library missing (e.g. a CPU-only run)
+        from scattersearch_b200 import graph
+        gt, _ = graph.bruteforce(X, Q, k, metric)
+        return gt.cpu().numpy(), {"kernel": f"torch ({e.__class__.__name__})"}
+    ids = torch.empty((nq, k), dtype=torch.int32, device=device)
+    st = torch.cuda.current_stream()
+    idx.bruteforce_device(Q, nq, k, ids, stream=st.cuda_stream)  # warm-up (norms, attributes)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    idx.bruteforce_device(Q, nq, k, ids, stream=st.cuda_stream)
+    b.record(st)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    idx.close()
+    return ids.cpu().numpy().view(np.uint32), {
+        "kernel": "bf_candidates_kernel (TF32 mma.sync, three-term products, FP32 accumulate) "
+                  "+ bf_rerank_kernel (exact FP32 distance, ties by id)",
+        "ms": ms, "tensor_tflops": 3 * 2 * nq * n * dim / ms / 1e9,
+        "queries": int(nq), "base": int(n)}
 
 
 def recall_at_10(ids, gt):
@@ -429,6 +458,22 @@ def measure_intra_latency(idx, wl, L, device, batches=(1, 4, 16), widths=(4, 8),
                                          wl["gt"][r * b:(r + 1) * b]))
             key = "plain" if W == 0 else f"intra_w{W}"
             row[key] = {"ms": float(np.median(ms)), "recall@10": float(np.mean(hits))}
+        for W in widths:  # ScatterSearch's own form: a pool per warp, election and ET
+            ms, hits = [], []
+            for r in range(reps):
+                q = Q[r * b:(r + 1) * b]
+                run = lambda: idx.search_scatter_device(q, b, K, L, W, ids, early_termination=True,
+                                                        seed=r + 1, stream=st.cuda_stream)
+                run()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                run()
+                e1.record(st)
+                torch.cuda.synchronize()
+                ms.append(e0.elapsed_time(e1))
+                hits.append(recall_at_10(ids.cpu().numpy().view(np.uint32),
+                                         wl["gt"][r * b:(r + 1) * b]))
+            row[f"scatter_et_w{W}"] = {"ms": float(np.median(ms)), "recall@10": float(np.mean(hits))}
         res.append(row)
         log(f"batch {b}: " + ", ".join(f"{k} {v['ms']:.2f} ms" for k, v in row.items()
                                           if k != "batch"))
@@ -582,6 +627,7 @@ def run_ours(args):
                    "l2": "inputs larger than L2 (base %.0f MB > 126 MB L2)"
                          % (wl["X"].numel() * 4 / 1e6),
                    "parallelism": f"replicas x{d.world}, queries sharded",
+                   "ground_truth": wl["gt_info"],
                    "tuning": {"warps_per_block": tune["warps_per_block"],
                               "hash_cap": tune["hash_cap"],
                               "sample": f"the {nq} bench queries (launch layout only)"}},

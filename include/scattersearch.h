@@ -191,14 +191,15 @@ int ss_batch_status(ss_index *h, uint32_t *failed_queries);
 int ss_search_batch_noalloc(ss_index *h, const float *queries, uint32_t nq, int K, int L,
                             uint32_t *ids, float *dists, void *stream);
 
-/* Replaces ANNSearch::MultiThreadSearchArraySimulation[WithET]
- * (src/annsearch.cpp:532-699, :839-1025): one query searched by a CTA of
- * `num_threads` warps (1..SS_MAX_INTRA_WIDTH), each step expanding the
- * num_threads best unexplored pool entries at once.  Acceptance, merge and
- * termination rules are those of ss_search, so num_threads == 1 returns
- * exactly the ss_search result; larger widths trade extra distance
- * evaluations for fewer dependent steps, as the reference's intra-query
- * threads do. */
+/* Several expansions per step for one query, keeping the plain search's
+ * rules: one CTA of `num_threads` warps (1..SS_MAX_INTRA_WIDTH) expands the
+ * num_threads best unexplored pool entries at once (the structure of the
+ * reference's ModifiedDeltaStepping, src/annsearch.cpp:1586-1731, with the
+ * acceptance, merge and termination rules of SearchArraySimulation).
+ * num_threads == 1 returns exactly the ss_search result; larger widths trade
+ * extra distance evaluations for fewer dependent steps, which lowers the
+ * latency of small batches.  ScatterSearch's own intra-query search is
+ * ss_search_scatter_batch below. */
 int ss_search_intra(ss_index *h, const float *query, int K, int L, int num_threads, uint32_t *ids,
                     float *dists);
 
@@ -211,6 +212,33 @@ int ss_search_intra_batch(ss_index *h, const float *queries, uint32_t nq, int K,
 int ss_search_intra_batch_device(ss_index *h, const float *queries, uint32_t nq, int K, int L,
                                  int num_threads, uint32_t *ids, float *dists, uint32_t *ndc,
                                  uint32_t *hops, void *stream);
+
+/* ScatterSearch's intra-query search itself: replaces
+ * ANNSearch::MultiThreadSearchArraySimulation (src/annsearch.cpp:532-699)
+ * and, with early_termination, MultiThreadSearchArraySimulationWithET
+ * (:839-1025, SearchUntilBestThreadStop :1368-1455).  One CTA per query;
+ * each of its num_threads warps (1..SS_SCATTER_MAX_WARPS) plays one
+ * reference thread: its own entry point and pool of L, one visited set
+ * shared by all, the pools' top K merged at the end.  Without early
+ * termination a pool is padded to L with random unvisited ids; with it, the
+ * warps vote at their 50th expansion, losers stop and continue from
+ * entries copied out of better warps' pools, and the winner's finish stops
+ * all.  Entry points and pads come from `seed` (the reference uses rand()).
+ * As with the reference's shared bitset, which warp reaches an id first
+ * decides where it lands, so results may differ between runs; they are
+ * measured by recall, not compared id for id.  L <= 512. */
+#define SS_SCATTER_MAX_WARPS 16
+int ss_search_scatter_batch(ss_index *h, const float *queries, uint32_t nq, int K, int L,
+                            int num_threads, int early_termination, uint64_t seed, uint32_t *ids,
+                            float *dists);
+
+/* Device-pointer form (asynchronous on `stream`); ndc / hops (nq uint32,
+ * may be NULL) receive each query's distance evaluations and expansions
+ * summed over its warps. */
+int ss_search_scatter_batch_device(ss_index *h, const float *queries, uint32_t nq, int K, int L,
+                                   int num_threads, int early_termination, uint64_t seed,
+                                   uint32_t *ids, float *dists, uint32_t *ndc, uint32_t *hops,
+                                   void *stream);
 
 /* Launch tuning of the batched warp-per-query kernel, normally chosen by the
  * autotuner (scattersearch_b200.autotune) per (dim, degree, L); no

@@ -90,26 +90,26 @@ class ANNSearch {
     flags.reset();
   }
 
-  // src/annsearch.cpp:532-699: num_threads warps expand num_threads
-  // candidates per step.
+  // ScatterSearch's intra-query search (src/annsearch.cpp:532-699): one warp
+  // per reference thread, each with its own entry point and pool, one shared
+  // visited set; entry points seeded from query_id.
   template <class Flags>
-  void MultiThreadSearchArraySimulation(const float *query, unsigned /*query_id*/, int K, int L,
+  void MultiThreadSearchArraySimulation(const float *query, unsigned query_id, int K, int L,
                                         int num_threads, Flags &flags,
                                         std::vector<unsigned> &indices) {
-    if ((int)indices.size() < K) indices.resize(K);
-    die_on_error(ss_search_intra(handle, query, K, L, num_threads,
-                                 reinterpret_cast<uint32_t *>(indices.data()), nullptr),
-                 handle, "MultiThreadSearchArraySimulation");
+    scatter(query, query_id, K, L, num_threads, 0, indices, "MultiThreadSearchArraySimulation");
     flags.reset();
   }
 
-  // src/annsearch.cpp:839-1025.  All warps of the CTA step in lock step, so
-  // there is no idle thread for the election / early termination to stop.
+  // With the election at the 50th expansion, early termination and stealing
+  // (src/annsearch.cpp:839-1025, :1368-1455).
   template <class Flags>
   void MultiThreadSearchArraySimulationWithET(const float *query, unsigned query_id, int K, int L,
                                               int num_threads, Flags &flags,
                                               std::vector<unsigned> &indices) {
-    MultiThreadSearchArraySimulation(query, query_id, K, L, num_threads, flags, indices);
+    scatter(query, query_id, K, L, num_threads, 1, indices,
+            "MultiThreadSearchArraySimulationWithET");
+    flags.reset();
   }
 
   // Batched extension: nq queries, one persistent launch.  ids: nq*K.
@@ -148,6 +148,16 @@ class ANNSearch {
     std::vector<uint32_t> out((size_t)base_num * rstride);
     die_on_error(ss_get_graph(handle, out.data(), rstride), handle, "graph_table");
     return out;
+  }
+
+ private:
+  void scatter(const float *query, unsigned query_id, int K, int L, int num_threads, int et,
+               std::vector<unsigned> &indices, const char *what) {
+    if ((int)indices.size() < K) indices.resize(K);
+    const uint64_t seed = (uint64_t)query_id * 0x9E3779B97F4A7C15ull + 1ull;
+    die_on_error(ss_search_scatter_batch(handle, query, 1, K, L, num_threads, et, seed,
+                                         reinterpret_cast<uint32_t *>(indices.data()), nullptr),
+                 handle, what);
   }
 
  public:

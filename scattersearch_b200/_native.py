@@ -20,6 +20,7 @@ STATUS_NAMES = {
 SS_MAX_L = 4096
 SS_MAX_DEGREE = 128
 SS_MAX_INTRA_WIDTH = 16
+SS_SCATTER_MAX_WARPS = 16
 SS_NOALLOC_MAX_QUERIES = 65536
 SS_NOALLOC_SCRATCH_BYTES = 256 + 4 * SS_NOALLOC_MAX_QUERIES
 
@@ -57,6 +58,10 @@ SIGNATURES = {
     "ss_search_intra_batch_device": (_i32, [_vp, _vp, _u32, _i32, _i32, _i32, _vp, _vp, _vp, _vp,
                                             _vp]),
     "ss_set_tuning": (_i32, [_vp, _i32, _i32, _i32]),
+    "ss_search_scatter_batch": (_i32, [_vp, _f32p, _u32, _i32, _i32, _i32, _i32, ctypes.c_uint64,
+                                       _u32p, _f32p]),
+    "ss_search_scatter_batch_device": (_i32, [_vp, _vp, _u32, _i32, _i32, _i32, _i32,
+                                              ctypes.c_uint64, _vp, _vp, _vp, _vp, _vp]),
     "ss_bruteforce": (_i32, [_vp, _f32p, _u32, _i32, _u32p, _f32p]),
     "ss_bruteforce_device": (_i32, [_vp, _vp, _u32, _i32, _vp, _vp, _vp]),
     "ss_server_create": (_i32, [_vp, _vp, _hp]),

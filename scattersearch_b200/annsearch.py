@@ -49,6 +49,11 @@ def _dptr(x):
     return ctypes.c_void_p(int(x)) if int(x) else None
 
 
+def _query_seed(query_id: int) -> int:
+    """Seed of the scatter search's entry points for one reference query id."""
+    return (int(query_id) * 0x9E3779B97F4A7C15 + 1) & 0xFFFFFFFFFFFFFFFF
+
+
 def _reset_flags(flags):
     if flags is not None and hasattr(flags, "reset"):
         flags.reset()
@@ -154,9 +159,12 @@ class ANNSearch:
     def MultiThreadSearchArraySimulation(self, query, query_id: int, K: int, L: int,
                                          num_threads: int, flags=None, indices=None):
         """ANNSearch::MultiThreadSearchArraySimulation (src/annsearch.cpp:532-699):
-        one query, ``num_threads`` warps expanding that many candidates per
-        step."""
-        ids, _ = self.search_intra(query, K, L, num_threads)
+        ScatterSearch's intra-query search with ``num_threads`` warps, each
+        with its own random entry point and pool, one shared visited set
+        (``search_scatter``).  The entry points are seeded from query_id."""
+        ids, _ = self.search_scatter(query, K, L, num_threads, early_termination=False,
+                                     seed=_query_seed(query_id))
+        ids = ids[0]
         if indices is not None:
             indices[:K] = ids.tolist() if isinstance(indices, list) else ids
         _reset_flags(flags)
@@ -165,12 +173,15 @@ class ANNSearch:
     def MultiThreadSearchArraySimulationWithET(self, query, query_id: int, K: int, L: int,
                                                num_threads: int, flags=None, indices=None):
         """ANNSearch::MultiThreadSearchArraySimulationWithET
-        (src/annsearch.cpp:839-1025).  The GPU CTA expands its warps' picks in
-        lock step, so no thread idles and the early-termination vote has
-        nothing to cut; this is the same call as
-        MultiThreadSearchArraySimulation."""
-        return self.MultiThreadSearchArraySimulation(query, query_id, K, L, num_threads, flags,
-                                                     indices)
+        (src/annsearch.cpp:839-1025): the scatter search with the election at
+        the 50th expansion, early termination and stealing."""
+        ids, _ = self.search_scatter(query, K, L, num_threads, early_termination=True,
+                                     seed=_query_seed(query_id))
+        ids = ids[0]
+        if indices is not None:
+            indices[:K] = ids.tolist() if isinstance(indices, list) else ids
+        _reset_flags(flags)
+        return ids
 
     # ------------------------------------------------------ numpy helpers
     def search(self, query, K: int, L: int):
@@ -227,6 +238,28 @@ class ANNSearch:
         self._check(self._lib.ss_bruteforce_device(
             self._h, _dptr(queries), int(nq), int(k), _dptr(ids), _dptr(dists),
             ctypes.c_void_p(int(stream)) if stream else None))
+
+    def search_scatter(self, queries, K: int, L: int, num_threads: int,
+                       early_termination: bool = False, seed: int = 1):
+        """ScatterSearch's intra-query search (MultiThreadSearchArraySimulation,
+        or WithET when ``early_termination``): one CTA per query, a pool per
+        warp, a shared visited set.  Returns (ids, dists), nq x K."""
+        q = _f32(queries).reshape(-1, self.dimension)
+        nq = q.shape[0]
+        ids = np.empty((nq, K), dtype=np.uint32)
+        dists = np.empty((nq, K), dtype=np.float32)
+        self._check(self._lib.ss_search_scatter_batch(
+            self._h, _ptr(q, _f32p), nq, int(K), int(L), int(num_threads),
+            int(bool(early_termination)), int(seed), _ptr(ids, _u32p), _ptr(dists, _f32p)))
+        return ids, dists
+
+    def search_scatter_device(self, queries, nq: int, K: int, L: int, num_threads: int, ids,
+                              dists=None, early_termination: bool = False, seed: int = 1,
+                              ndc=None, hops=None, stream=None):
+        self._check(self._lib.ss_search_scatter_batch_device(
+            self._h, _dptr(queries), int(nq), int(K), int(L), int(num_threads),
+            int(bool(early_termination)), int(seed), _dptr(ids), _dptr(dists), _dptr(ndc),
+            _dptr(hops), ctypes.c_void_p(int(stream)) if stream else None))
 
     def search_intra(self, query, K: int, L: int, num_threads: int):
         q = _f32(query).reshape(-1)

@@ -324,6 +324,46 @@ int launch_intra(ss_index *h, SearchCtx *c, const float *d_q, uint32_t nq, int K
   return SS_OK;
 }
 
+int launch_scatter(ss_index *h, SearchCtx *c, const float *d_q, uint32_t nq, int K, int L, int W,
+                   int et, uint64_t seed, uint32_t *d_ids, float *d_dists, uint32_t *d_ndc,
+                   uint32_t *d_hops, cudaStream_t stream) {
+  ssb::GraphView g = h->view();
+  ssb::SmemPlan plan = ssb::plan_scatter_smem(g, L, W);
+  if (ssb::scatter_smem_bytes(plan, W) > 227 * 1024)
+    return set_err(h, SS_ERR_UNSUPPORTED, "L=%d with %d warps needs %zu bytes of shared memory",
+                   L, W, ssb::scatter_smem_bytes(plan, W));
+  SS_CUDA(h, c->spill.ensure((size_t)std::max(nq, 1u) * spill_words(h) * 4, true),
+          "spill bitset allocation");
+  SS_CUDA(h, c->status.ensure((size_t)std::max(nq, 1u) * 4), "status allocation");
+  ssb::BatchArgs a{};
+  a.queries = d_q;
+  a.qstride = h->dim;
+  a.nq = nq;
+  a.K0 = K;
+  a.L0 = L;
+  a.ids = d_ids;
+  a.dists = d_dists;
+  a.ndc = d_ndc;
+  a.hops = d_hops;
+  a.status = c->status.as<int32_t>();
+  a.spill_bits = c->spill.as<uint32_t>();
+  a.spill_words = spill_words(h);
+  a.max_hops = h->n + 1;
+  SS_CUDA(h, cudaMemsetAsync(c->status.p, 0, (size_t)nq * 4, stream), "status reset");
+  SS_CUDA(h, ssb::launch_scatter_search(g, a, plan, W, et, seed, stream), "scatter launch");
+  return SS_OK;
+}
+
+int check_scatter_args(ss_index *h, int K, int L, int W) {
+  int rc = check_search_args(h, K, L);
+  if (rc) return rc;
+  if (W < 1 || W > SS_SCATTER_MAX_WARPS)
+    return set_err(h, SS_ERR_INVALID_ARGUMENT, "num_threads=%d outside 1..%d", W,
+                   SS_SCATTER_MAX_WARPS);
+  if (L > 512) return set_err(h, SS_ERR_UNSUPPORTED, "the scatter search takes L <= 512");
+  return SS_OK;
+}
+
 int upload_graph(ss_index *h, const std::vector<uint32_t> &adj, uint32_t rstride, uint32_t ep,
                  uint32_t max_deg) {
   DeviceGuard dg(h->device);
@@ -894,6 +934,55 @@ int ss_bruteforce_device(ss_index *h, const float *queries, uint32_t nq, int k, 
   std::lock_guard<std::mutex> lk(h->dev_mu);
   return bruteforce_common(h, &h->dev_ctx, queries, h->dim, nq, k, ids, dists,
                            static_cast<cudaStream_t>(stream));
+}
+
+int ss_search_scatter_batch(ss_index *h, const float *queries, uint32_t nq, int K, int L,
+                            int num_threads, int early_termination, uint64_t seed, uint32_t *ids,
+                            float *dists) {
+  int rc = check_scatter_args(h, K, L, num_threads);
+  if (rc) return rc;
+  if (nq == 0) return SS_OK;
+  if (!queries || !ids) return set_err(h, SS_ERR_INVALID_ARGUMENT, "null queries or ids");
+  DeviceGuard dg(h->device);
+  CtxLease lease(h);
+  SearchCtx *c = lease.c;
+  if (!c) return set_err(h, SS_ERR_CUDA, "cannot create a stream");
+  const size_t total = (size_t)nq * K;
+  SS_CUDA(h, c->q.ensure((size_t)nq * h->dim * 4), "query buffer");
+  SS_CUDA(h, c->ids.ensure(total * 4), "ids buffer");
+  SS_CUDA(h, c->dists.ensure(total * 4), "dists buffer");
+  SS_CUDA(h, cudaMemcpyAsync(c->q.p, queries, (size_t)nq * h->dim * 4, cudaMemcpyHostToDevice,
+                             c->stream),
+          "query upload");
+  rc = launch_scatter(h, c, c->q.as<float>(), nq, K, L, num_threads, early_termination, seed,
+                      c->ids.as<uint32_t>(), c->dists.as<float>(), nullptr, nullptr, c->stream);
+  if (rc) return rc;
+  c->h_status.resize(nq);
+  SS_CUDA(h, cudaMemcpyAsync(ids, c->ids.p, total * 4, cudaMemcpyDeviceToHost, c->stream),
+          "ids download");
+  if (dists)
+    SS_CUDA(h, cudaMemcpyAsync(dists, c->dists.p, total * 4, cudaMemcpyDeviceToHost, c->stream),
+            "dists download");
+  SS_CUDA(h, cudaMemcpyAsync(c->h_status.data(), c->status.p, (size_t)nq * 4,
+                             cudaMemcpyDeviceToHost, c->stream),
+          "status download");
+  SS_CUDA(h, cudaStreamSynchronize(c->stream), "scatter search");
+  return status_to_error(h, c->h_status.data(), nq);
+}
+
+int ss_search_scatter_batch_device(ss_index *h, const float *queries, uint32_t nq, int K, int L,
+                                   int num_threads, int early_termination, uint64_t seed,
+                                   uint32_t *ids, float *dists, uint32_t *ndc, uint32_t *hops,
+                                   void *stream) {
+  int rc = check_scatter_args(h, K, L, num_threads);
+  if (rc) return rc;
+  if (nq == 0) return SS_OK;
+  if (!queries || !ids) return set_err(h, SS_ERR_INVALID_ARGUMENT, "null queries or ids");
+  DeviceGuard dg(h->device);
+  std::lock_guard<std::mutex> lk(h->dev_mu);
+  h->dev_last_nq = nq;
+  return launch_scatter(h, &h->dev_ctx, queries, nq, K, L, num_threads, early_termination, seed,
+                        ids, dists, ndc, hops, static_cast<cudaStream_t>(stream));
 }
 
 int ss_batch_status(ss_index *h, uint32_t *failed_queries) {

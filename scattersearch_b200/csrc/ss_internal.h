@@ -77,6 +77,13 @@ cudaError_t launch_warp_search(const GraphView &g, const BatchArgs &a, const Sme
 cudaError_t launch_intra_search(const GraphView &g, const BatchArgs &a, const SmemPlan &p,
                                 int width, cudaStream_t stream);
 
+// ScatterSearch's intra-query search: one CTA of `width` warps per query,
+// each warp with its own pool (et: election and early termination).
+SmemPlan plan_scatter_smem(const GraphView &g, int L_max, int width);
+size_t scatter_smem_bytes(const SmemPlan &p, int width);
+cudaError_t launch_scatter_search(const GraphView &g, const BatchArgs &a, const SmemPlan &p,
+                                  int width, int et, uint64_t seed, cudaStream_t stream);
+
 // Resident CTAs per SM for the warp kernel with this plan (0 if it cannot run).
 int warp_search_occupancy(const GraphView &g, const SmemPlan &p, int warps_per_block);
 

@@ -25,6 +25,7 @@
 #include <set>
 #include <utility>
 
+#include "scattersearch.h"
 #include "ss_distance.cuh"
 #include "ss_internal.h"
 
@@ -473,6 +474,103 @@ __device__ __forceinline__ void accepted_positions(const WarpSmem &s, int na, in
   }
 }
 
+// Step 4 of a hop: candidates cid/ckey[0..nc) (adjacency order) with key
+// below the hop's threshold are accepted, in order, into ak/aid/acle with
+// their pool rank (entries <= key).  With check_dups, a candidate whose id is
+// already in the pool under the same key is dropped.  Returns the count.
+template <int RCH>
+__device__ __forceinline__ int accept_candidates(const WarpSmem &s, int nc, int size, uint32_t thr,
+                                                 bool check_dups, int lane) {
+  const unsigned lanemask_lt = (1u << lane) - 1u;
+  const int top = floor_pow2(size);
+  int na = 0;
+#pragma unroll
+  for (int c = 0; c < RCH; ++c) {
+    const int e = c * 32 + lane;
+    const uint32_t key = e < nc ? s.ckey[e] : 0xFFFFFFFFu;
+    bool acc = e < nc && key < thr;
+    int cle = 0;
+    uint32_t id = 0;
+    if (acc) {
+      id = s.cid[e];
+      cle = count_le_bf(s.pk, size, top, key);
+      if (check_dups) {
+        for (int j = cle - 1; j >= 0 && s.pk[j] == key; --j) {
+          if ((s.pid[j] & ~kExplored) == id) {
+            acc = false;
+            break;
+          }
+        }
+      }
+    }
+    const unsigned am = __ballot_sync(kFull, acc);
+    if (acc) {
+      const int pos = na + __popc(am & lanemask_lt);
+      s.ak[pos] = key;
+      s.aid[pos] = id;
+      s.acle[pos] = (uint32_t)cle;
+    }
+    na += __popc(am);
+  }
+  return na;
+}
+
+// Step 5 of a hop: stable in-place merge of the na accepted candidates
+// (slots npos, from accepted_positions) into the pool of `size` entries,
+// truncated to L.  Old entries at and after p0 move up by the number of new
+// keys below them, in 128-entry windows from the top down, 4 entries per
+// lane, each window fully read before it is written; then the new entries go
+// to their slots.  `size` becomes min(L, size + na).
+template <int RCH>
+__device__ __forceinline__ void merge_accepted(const WarpSmem &s, int &size, int na, int p0, int L,
+                                               const uint32_t (&nkey)[RCH],
+                                               const uint32_t (&nid)[RCH], const int (&npos)[RCH],
+                                               int lane) {
+  for (int w = ((size - 1) >> 7) << 7; w + 128 > p0 && w >= 0; w -= 128) {
+    const int j0 = w + 4 * lane;
+    const bool any = j0 + 3 >= p0 && j0 < size;
+    uint4 kk = make_uint4(0, 0, 0, 0), ii = make_uint4(0, 0, 0, 0);
+    if (any) {
+      kk = *reinterpret_cast<const uint4 *>(s.pk + j0);
+      ii = *reinterpret_cast<const uint4 *>(s.pid + j0);
+    }
+    int c0 = 0, c1 = 0, c2 = 0, c3 = 0;
+#pragma unroll 4
+    for (int i = 0; i < na; ++i) {
+      const uint32_t sv = s.ak[i];
+      c0 += kk.x > sv;
+      c1 += kk.y > sv;
+      c2 += kk.z > sv;
+      c3 += kk.w > sv;
+    }
+    __syncwarp();
+    if (any) {
+      const uint32_t ks[4] = {kk.x, kk.y, kk.z, kk.w};
+      const uint32_t is[4] = {ii.x, ii.y, ii.z, ii.w};
+      const int cs[4] = {c0, c1, c2, c3};
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int j = j0 + t;
+        const int dst = j + cs[t];
+        if (j >= p0 && j < size && dst < L) {
+          s.pk[dst] = ks[t];
+          s.pid[dst] = is[t];
+        }
+      }
+    }
+    __syncwarp();
+  }
+#pragma unroll
+  for (int c = 0; c < RCH; ++c) {
+    if (npos[c] < L) {
+      s.pk[npos[c]] = nkey[c];
+      s.pid[npos[c]] = nid[c];
+    }
+  }
+  __syncwarp();
+  size = min(L, size + na);
+}
+
 // One query, one warp.  Each hop (batch-merge form of annsearch.cpp:218-253):
 //   1. expand pool slot k, the first unexplored one (known from the previous
 //      hop); u is the unexplored slot after it;
@@ -644,36 +742,7 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
     // 4. acceptance in adjacency order, with each key's pool rank; after an
     //    eviction, a candidate already in the pool (same id under the same
     //    key) is dropped
-    const int top = floor_pow2(size);
-    int na = 0;
-#pragma unroll
-    for (int c = 0; c < RCH; ++c) {
-      const int e = c * 32 + lane;
-      const uint32_t key = e < nc ? s.ckey[e] : 0xFFFFFFFFu;
-      bool acc = e < nc && key < thr;
-      int cle = 0;
-      uint32_t id = 0;
-      if (acc) {
-        id = s.cid[e];
-        cle = count_le_bf(s.pk, size, top, key);
-        if (vis.lossy) {
-          for (int j = cle - 1; j >= 0 && s.pk[j] == key; --j) {
-            if ((s.pid[j] & ~kExplored) == id) {
-              acc = false;
-              break;
-            }
-          }
-        }
-      }
-      const unsigned am = __ballot_sync(kFull, acc);
-      if (acc) {
-        const int pos = na + __popc(am & lanemask_lt);
-        s.ak[pos] = key;
-        s.aid[pos] = id;
-        s.acle[pos] = (uint32_t)cle;
-      }
-      na += __popc(am);
-    }
+    const int na = accept_candidates<RCH>(s, nc, size, thr, vis.lossy, lane);
     if (na == 0) {
       pref_node = unode;
       if (unode != kNoneId) load_row<RCH>(g, unode, lane, pref_row);
@@ -704,53 +773,8 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
       k = (u >= 0 && u < p0) ? u : p0;
     }
 
-    // 5. stable merge into the pool, in place: old entries at and after p0
-    //    move up by the number of new keys below them, in 128-entry windows
-    //    from the top down, 4 entries per lane, each window fully read before
-    //    it is written; then the new entries go to their slots.
-    for (int w = ((size - 1) >> 7) << 7; w + 128 > p0 && w >= 0; w -= 128) {
-      const int j0 = w + 4 * lane;
-      const bool any = j0 + 3 >= p0 && j0 < size;
-      uint4 kk = make_uint4(0, 0, 0, 0), ii = make_uint4(0, 0, 0, 0);
-      if (any) {
-        kk = *reinterpret_cast<const uint4 *>(s.pk + j0);
-        ii = *reinterpret_cast<const uint4 *>(s.pid + j0);
-      }
-      int c0 = 0, c1 = 0, c2 = 0, c3 = 0;
-#pragma unroll 4
-      for (int i = 0; i < na; ++i) {
-        const uint32_t sv = s.ak[i];
-        c0 += kk.x > sv;
-        c1 += kk.y > sv;
-        c2 += kk.z > sv;
-        c3 += kk.w > sv;
-      }
-      __syncwarp();
-      if (any) {
-        const uint32_t ks[4] = {kk.x, kk.y, kk.z, kk.w};
-        const uint32_t is[4] = {ii.x, ii.y, ii.z, ii.w};
-        const int cs[4] = {c0, c1, c2, c3};
-#pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          const int j = j0 + t;
-          const int dst = j + cs[t];
-          if (j >= p0 && j < size && dst < L) {
-            s.pk[dst] = ks[t];
-            s.pid[dst] = is[t];
-          }
-        }
-      }
-      __syncwarp();
-    }
-#pragma unroll
-    for (int c = 0; c < RCH; ++c) {
-      if (npos[c] < L) {
-        s.pk[npos[c]] = nkey[c];
-        s.pid[npos[c]] = nid[c];
-      }
-    }
-    __syncwarp();
-    size = min(L, size + na);
+    // 5. stable merge into the pool (older entries first on ties)
+    merge_accepted<RCH>(s, size, na, p0, L, nkey, nid, npos, lane);
   }
 
   // Results: slots the pool never filled keep the reference's value-
@@ -1184,6 +1208,455 @@ __global__ void __launch_bounds__(512) intra_search_kernel(GraphView g, BatchArg
   }
 }
 
+// ------------------------------------------- scatter: independent pools ---
+// ScatterSearch's intra-query search (MultiThreadSearchArraySimulation,
+// src/annsearch.cpp:532-699, and its election variant
+// MultiThreadSearchArraySimulationWithET, :839-1025 with
+// SearchUntilBestThreadStop, :1368-1455).  One CTA per query, one warp per
+// reference thread.  Each warp starts from its own entry point and runs the
+// plain best-first loop on its own pool of L; all warps share one exact
+// visited set, so whichever warp meets an id first owns it (as with the
+// reference's shared bitset, results depend on the warps' timing and are
+// judged by recall).  At the end the pools' top K are merged, duplicates
+// dropped.
+//   plain  the pool starts with every neighbour of the entry point and is
+//          padded to L with random unvisited ids (:552-575);
+//   ET     the pool starts with the neighbours only; at the warp's 50th
+//          expansion it votes with its K-th distance; once all have voted,
+//          warps whose best entry is worse than the winning vote stop and
+//          (like the others that finish early) continue from unexplored
+//          entries copied out of a "good" warp's pool; the winner finishing
+//          stops every warp (:858-999, :1368-1455).
+// Entry points and pads come from a counter-based hash of (seed, query, warp)
+// instead of rand(); the election's ties go to the lower warp; and copies out
+// of another warp's pool are taken under that pool's sequence counter, where
+// the reference reads them unsynchronised.
+constexpr int kMaxScatter = SS_SCATTER_MAX_WARPS;
+constexpr int kElectionHop = 50;
+
+struct ScatterCtl {
+  unsigned long long best;  // (K-th key at the election hop) << 32 | warp
+  int decided;              // warps that voted
+  int finish;               // the elected warp finished: all stop
+  int vis_count;            // entries reserved in the visited hash
+  int vis_spilled;          // hash full: new ids go to the global bitset
+  int status;
+  unsigned ndc, hops;
+  int good[kMaxScatter];          // 1: pool head better than the winning vote
+  int reached[kMaxScatter];       // voted
+  unsigned version[kMaxScatter];  // pool sequence counters (odd while changing)
+  int size[kMaxScatter];          // pool sizes
+};
+
+// Shared state that other warps change is read by lane 0 and broadcast, so
+// every lane of a warp takes the same branch (warp-wide collectives follow).
+__device__ __forceinline__ int uniform_load(const int *p, int lane) {
+  int v = 0;
+  if (lane == 0) v = *(const volatile int *)p;
+  return __shfl_sync(kFull, v, 0);
+}
+__device__ __forceinline__ unsigned uniform_load(const unsigned *p, int lane) {
+  unsigned v = 0;
+  if (lane == 0) v = *(const volatile unsigned *)p;
+  return __shfl_sync(kFull, v, 0);
+}
+__device__ __forceinline__ unsigned long long uniform_load(const unsigned long long *p, int lane) {
+  unsigned long long v = 0;
+  if (lane == 0) v = *(const volatile unsigned long long *)p;
+  const unsigned lo = __shfl_sync(kFull, (unsigned)v, 0);
+  const unsigned hi = __shfl_sync(kFull, (unsigned)(v >> 32), 0);
+  return ((unsigned long long)hi << 32) | lo;
+}
+
+__device__ __forceinline__ uint32_t scatter_rng(uint64_t seed, uint32_t q, uint32_t w,
+                                                uint32_t i) {
+  uint64_t x = seed ^ ((uint64_t)q << 32) ^ ((uint64_t)w << 20) ^ (uint64_t)i;
+  x += 0x9E3779B97F4A7C15ull;  // splitmix64 finaliser
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return (uint32_t)((x ^ (x >> 31)) >> 32);
+}
+
+// Reserves room for up to `m` new ids in the shared visited hash; switches
+// this warp (and, through ctl, the others) to spilling once the hash is full.
+__device__ __forceinline__ void scatter_reserve(Visited &v, ScatterCtl *ctl, int m, int lane) {
+  if (v.spilled) return;
+  int r = 0;
+  if (lane == 0) r = atomicAdd(&ctl->vis_count, m);
+  r = __shfl_sync(kFull, r, 0);
+  if ((uint32_t)(r + m) > v.limit) {
+    if (lane == 0) atomicExch(&ctl->vis_spilled, 1);
+    v.spilled = true;
+  } else if (uniform_load(&ctl->vis_spilled, lane)) {
+    v.spilled = true;
+  }
+}
+
+// Copies up to `cap` unexplored entries of warp t's pool, taken from its end
+// (as SearchUntilBestThreadStop does), into this warp's cid/ckey; returns how
+// many, or 0 when the pool changed under every attempt.
+__device__ __forceinline__ int scatter_copy_unexplored(const WarpSmem &src, ScatterCtl *ctl, int t,
+                                                       const WarpSmem &dst, int cap, int lane) {
+  const unsigned lanemask_lt = (1u << lane) - 1u;
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    const unsigned v0 = uniform_load(&ctl->version[t], lane);
+    if (v0 & 1u) continue;
+    __threadfence_block();
+    const int sz = uniform_load(&ctl->size[t], lane);
+    int got = 0;
+    for (int b = sz - 1; b >= 1 && got < cap; b -= 32) {
+      const int j = b - lane;
+      uint32_t id = 0, key = 0;
+      bool un = false;
+      if (j >= 1) {
+        id = *(volatile uint32_t *)&src.pid[j];
+        key = *(volatile uint32_t *)&src.pk[j];
+        un = !(id & kExplored);
+      }
+      const unsigned m = __ballot_sync(kFull, un);
+      const int pos = got + __popc(m & lanemask_lt);
+      if (un && pos < cap) {
+        dst.cid[pos] = id;
+        dst.ckey[pos] = key;
+      }
+      got = min(cap, got + __popc(m));
+    }
+    __threadfence_block();
+    const unsigned v1 = uniform_load(&ctl->version[t], lane);
+    if (v0 == v1) return got;
+  }
+  return 0;
+}
+
+template <int NB, int RCH, int PITEMS>
+__global__ void __launch_bounds__(512) scatter_search_kernel(GraphView g, BatchArgs a, SmemPlan p,
+                                                             int W, int et, uint64_t seed) {
+  extern __shared__ __align__(128) uint32_t smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned lanemask_lt = (1u << lane) - 1u;
+  const uint32_t q_idx = blockIdx.x;
+  if (q_idx >= a.nq) return;
+  const int K = a.Ks ? a.Ks[q_idx] : a.K0;
+  const int L = a.Ls ? a.Ls[q_idx] : a.L0;
+  const int64_t off = a.out_off ? a.out_off[q_idx] : (int64_t)q_idx * a.K0;
+  if (K < 1 || K > L || L > (int)p.pool_cap) {
+    if (threadIdx.x == 0 && a.status) a.status[q_idx] = kStatusBadArgs;
+    return;
+  }
+  // shared: query, visited hash, control block; then one pool region per warp
+  float *qs = reinterpret_cast<float *>(smem);
+  uint32_t *tab = smem + p.q_words;
+  ScatterCtl *ctl = reinterpret_cast<ScatterCtl *>(tab + p.hash_cap);
+  uint32_t *wbase = tab + p.hash_cap + p.step_cap;  // step_cap: words of ScatterCtl
+  auto carve = [&](int w) {
+    WarpSmem s{};
+    uint32_t *b = wbase + (size_t)w * p.words_per_team;
+    s.q = qs;
+    s.pk = b;
+    b += p.pool_cap;
+    s.pid = b;
+    b += p.pool_cap;
+    s.cid = b;
+    b += p.cand_cap;
+    s.ckey = b;
+    b += p.cand_cap;
+    s.ak = b;
+    b += p.cand_cap;
+    s.aid = b;
+    b += p.cand_cap;
+    s.acle = b;
+    return s;
+  };
+  const WarpSmem s = carve(warp);
+  const float *qsrc = a.queries + (size_t)q_idx * a.qstride;
+  const int qw = (int)g.nb * 8;
+  for (int i = threadIdx.x; i < qw; i += blockDim.x) qs[i] = i < (int)g.dim ? qsrc[i] : 0.f;
+  for (uint32_t i = threadIdx.x; i < p.hash_cap; i += blockDim.x) tab[i] = kNoneId;
+  if (threadIdx.x == 0) {
+    ctl->best = ~0ull;
+    ctl->decided = 0;
+    ctl->finish = 0;
+    ctl->vis_count = 0;
+    ctl->vis_spilled = 0;
+    ctl->status = kStatusOk;
+    ctl->ndc = 0;
+    ctl->hops = 0;
+  }
+  if (threadIdx.x < kMaxScatter) {
+    ctl->good[threadIdx.x] = 0;
+    ctl->reached[threadIdx.x] = 0;
+    ctl->version[threadIdx.x] = 0;
+    ctl->size[threadIdx.x] = 0;
+  }
+  __syncthreads();
+
+  Visited vis;
+  vis.tab = tab;
+  vis.mask = p.hash_cap - 1;
+  vis.log2cap = p.hash_log2;
+  vis.limit = p.hash_limit;
+  vis.count = 0;
+  vis.bits = a.spill_bits ? a.spill_bits + (size_t)q_idx * a.spill_words : nullptr;
+  vis.spilled = false;
+  uint32_t ndc = 0, hops = 0;
+  int32_t status = kStatusOk;
+
+  // --- initial pool
+  int size = 0;
+  {
+    const uint32_t ep = scatter_rng(seed, q_idx, warp, 0) % g.n;
+    uint32_t row[RCH];
+    load_row<RCH>(g, ep, lane, row);
+    scatter_reserve(vis, ctl, (int)g.rstride, lane);
+#pragma unroll
+    for (int c = 0; c < RCH; ++c) {
+      const int m = c * 32 + lane;
+      const bool valid = row[c] != kNoneId && m < L;
+      if (valid) {
+        s.pid[m] = row[c];
+        visit(vis, row[c]);
+      }
+      size += __popc(__ballot_sync(kFull, valid));
+    }
+    if (!et) {
+      // pad to L with random ids nobody has visited (claimed atomically)
+      scatter_reserve(vis, ctl, L - size, lane);
+      for (uint32_t round = 0; size < L && round < 64; ++round) {
+        const int need = L - size;
+        uint32_t id = scatter_rng(seed, q_idx, warp, 1 + round * 32 + lane) % g.n;
+        bool got = false;
+        if (lane < need) {
+          for (uint32_t probe = 0; probe < 64 && !got; ++probe) {
+            got = visit(vis, id);
+            if (!got) id = id + 1 == g.n ? 0 : id + 1;
+          }
+        }
+        const unsigned gm = __ballot_sync(kFull, got);
+        if (got) s.pid[size + __popc(gm & lanemask_lt)] = id;
+        size += __popc(gm);
+      }
+    }
+    if (vis.spilled && !vis.bits) status = kStatusVisitedFull;
+    __syncwarp();
+    eval_candidates<NB>(g, qs, s.pid, s.pk, size, lane);
+    ndc += size;
+    __syncwarp();
+    // sort by (key, position)
+    uint64_t x[PITEMS];
+#pragma unroll
+    for (int i = 0; i < PITEMS; ++i) {
+      const int e = i * 32 + lane;
+      x[i] = e < size ? (((uint64_t)s.pk[e] << 32) | (uint32_t)e) : kInvalidKey;
+    }
+    warp_sort<PITEMS>(x, lane);
+    uint32_t sid[PITEMS];
+#pragma unroll
+    for (int i = 0; i < PITEMS; ++i) {
+      const int e = i * 32 + lane;
+      sid[i] = e < size ? s.pid[(uint32_t)x[i]] : 0u;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < PITEMS; ++i) {
+      const int e = i * 32 + lane;
+      if (e < size) {
+        s.pk[e] = (uint32_t)(x[i] >> 32);
+        s.pid[e] = sid[i];
+      }
+    }
+    __syncwarp();
+    if (lane == 0) ctl->size[warp] = size;
+  }
+
+  // --- best-first loop, then (ET) stealing rounds
+  bool voted = false, need_identify = true, dup_check = false;
+  const bool is_et = et != 0;
+  for (int phase = 0; phase < 2 && status == kStatusOk; ++phase) {
+    if (phase == 1) {
+      // ET: a warp that is not the winner continues from unexplored entries
+      // of good warps while the winner runs (SearchUntilBestThreadStop)
+      if (!is_et || uniform_load(&ctl->finish, lane)) break;
+      const unsigned long long best = uniform_load(&ctl->best, lane);
+      if (best != ~0ull && (int)(best & 0xFFFFFFFFu) == warp) break;
+      int target = -1;
+      for (int round = 0; round < 10 && target < 0; ++round) {
+        const int t = (int)(scatter_rng(seed, q_idx, warp, 100000u + round) % (uint32_t)W);
+        if (t != warp && uniform_load(&ctl->reached[t], lane) && uniform_load(&ctl->good[t], lane))
+          target = t;
+      }
+      if (target < 0) break;
+      dup_check = true;
+      const WarpSmem src = carve(target);
+      const int got = scatter_copy_unexplored(src, ctl, target, s, (int)p.cand_cap, lane);
+      if (got > 0 && size > 0) {
+        __syncwarp();
+        const uint32_t thr = s.pk[size - 1];
+        const int na = accept_candidates<RCH>(s, got, size, thr, true, lane);
+        if (na > 0) {
+          __syncwarp();
+          uint32_t nkey[RCH], nid[RCH];
+          int npos[RCH];
+          accepted_positions<RCH>(s, na, lane, nkey, nid, npos, size);
+          int pmin = npos[0];
+#pragma unroll
+          for (int c = 1; c < RCH; ++c) pmin = min(pmin, npos[c]);
+          const int p0 = (int)__reduce_min_sync(kFull, (uint32_t)pmin);
+          if (lane == 0) atomicAdd(&ctl->version[warp], 1u);
+          __threadfence_block();
+          int sz = size;
+          merge_accepted<RCH>(s, sz, na, p0, size, nkey, nid, npos, lane);  // size kept
+          __threadfence_block();
+          if (lane == 0) atomicAdd(&ctl->version[warp], 1u);
+        }
+      }
+    }
+    for (;;) {
+      if (is_et) {
+        if (uniform_load(&ctl->finish, lane)) break;
+        if (hops == (uint32_t)kElectionHop && !voted) {
+          voted = true;
+          const uint32_t kth = size >= K ? s.pk[K - 1] : 0xFFFFFFFFu;
+          if (lane == 0) {
+            atomicMin(&ctl->best, ((unsigned long long)kth << 32) | (unsigned)warp);
+            ctl->reached[warp] = 1;
+            __threadfence_block();
+            atomicAdd(&ctl->decided, 1);
+          }
+          __syncwarp();
+        }
+        if (need_identify && uniform_load(&ctl->decided, lane) == W) {
+          need_identify = false;
+          const unsigned long long best = uniform_load(&ctl->best, lane);
+          const uint32_t bk = (uint32_t)(best >> 32);
+          if (size > 0 && bk < s.pk[0]) break;                      // a losing warp stops
+          if (size > 0 && bk > s.pk[0] && lane == 0) ctl->good[warp] = 1;
+        }
+      }
+      // first unexplored slot
+      int k = -1;
+      for (int b0 = 0; b0 < size; b0 += 32) {
+        const int idx = b0 + lane;
+        const bool un = idx < size && !(s.pid[idx] & kExplored);
+        const unsigned bm = __ballot_sync(kFull, un);
+        if (bm) {
+          k = b0 + __ffs(bm) - 1;
+          break;
+        }
+      }
+      if (k < 0) break;
+      if (hops >= a.max_hops) {
+        status = kStatusHopLimit;
+        break;
+      }
+      const uint32_t node = s.pid[k];
+      const uint32_t thr = s.pk[size - 1];
+      __syncwarp();
+      if (lane == 0) s.pid[k] = node | kExplored;
+      ++hops;
+      uint32_t row[RCH];
+      load_row<RCH>(g, node, lane, row);
+      scatter_reserve(vis, ctl, (int)g.rstride, lane);
+      if (vis.spilled && !vis.bits) {
+        status = kStatusVisitedFull;
+        break;
+      }
+      int nc = 0;
+#pragma unroll
+      for (int c = 0; c < RCH; ++c) {
+        const bool valid = row[c] != kNoneId;
+        const unsigned peers = __match_any_sync(kFull, row[c]);
+        const bool leader = valid && (peers & lanemask_lt) == 0u;
+        const bool fresh = leader && visit(vis, row[c]);
+        const unsigned fm = __ballot_sync(kFull, fresh);
+        if (fresh) s.cid[nc + __popc(fm & lanemask_lt)] = row[c];
+        nc += __popc(fm);
+      }
+      if (nc == 0) continue;
+      __syncwarp();
+      eval_candidates<NB>(g, qs, s.cid, s.ckey, nc, lane);
+      ndc += nc;
+      __syncwarp();
+      const int na = accept_candidates<RCH>(s, nc, size, thr, dup_check, lane);
+      if (na == 0) continue;
+      __syncwarp();
+      uint32_t nkey[RCH], nid[RCH];
+      int npos[RCH];
+      accepted_positions<RCH>(s, na, lane, nkey, nid, npos, L);
+      int pmin = npos[0];
+#pragma unroll
+      for (int c = 1; c < RCH; ++c) pmin = min(pmin, npos[c]);
+      const int p0 = (int)__reduce_min_sync(kFull, (uint32_t)pmin);
+      if (lane == 0) atomicAdd(&ctl->version[warp], 1u);
+      __threadfence_block();
+      merge_accepted<RCH>(s, size, na, p0, L, nkey, nid, npos, lane);
+      __threadfence_block();
+      if (lane == 0) {
+        ctl->size[warp] = size;
+        atomicAdd(&ctl->version[warp], 1u);
+      }
+    }
+    if (phase == 0 && is_et) {
+      // the winner finishing stops everyone
+      const unsigned long long best = uniform_load(&ctl->best, lane);
+      if (best != ~0ull && (int)(best & 0xFFFFFFFFu) == warp && lane == 0)
+        atomicExch(&ctl->finish, 1);
+    }
+  }
+  if (lane == 0) {
+    atomicAdd(&ctl->ndc, ndc);
+    atomicAdd(&ctl->hops, hops);
+    if (status != kStatusOk) atomicExch(&ctl->status, status);
+  }
+  __syncthreads();
+
+  // --- merge: the K best of all pools, one copy per id (warp 0; lane w
+  // follows pool w)
+  if (warp == 0) {
+    uint32_t *oid = a.ids + off;
+    float *od = a.dists ? a.dists + off : nullptr;
+    const WarpSmem mine = carve(lane < W ? lane : 0);
+    const int msize = lane < W ? ctl->size[lane] : 0;
+    int head = 0, out = 0;
+    uint32_t last = kNoneId;
+    while (out < K) {
+      const uint64_t v = head < msize ? (((uint64_t)mine.pk[head] << 32) |
+                                         (mine.pid[head] & ~kExplored))
+                                      : kInvalidKey;
+      uint64_t mn = v;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const uint64_t other = shfl_xor_u64(mn, o);
+        mn = other < mn ? other : mn;
+      }
+      if (mn == kInvalidKey) break;
+      const unsigned who = __ballot_sync(kFull, v == mn);
+      if (lane == __ffs(who) - 1) ++head;
+      const uint32_t id = (uint32_t)mn;
+      if (id != last) {
+        if (lane == 0) {
+          oid[out] = id;
+          if (od) od[out] = key_to_float((uint32_t)(mn >> 32));
+        }
+        ++out;
+        last = id;
+      }
+    }
+    for (int i = out + lane; i < K; i += 32) {
+      oid[i] = 0u;
+      if (od) od[i] = 0.f;
+    }
+  }
+  if (ctl->vis_spilled && vis.bits) {
+    __syncthreads();
+    for (uint32_t w = threadIdx.x; w < a.spill_words; w += blockDim.x) vis.bits[w] = 0u;
+  }
+  if (threadIdx.x == 0) {
+    if (a.ndc) a.ndc[q_idx] = ctl->ndc;
+    if (a.hops) a.hops[q_idx] = ctl->hops;
+    if (a.status) a.status[q_idx] = ctl->status;
+  }
+}
+
 // ----------------------------------------------------------- dispatch ---
 using WarpFn = void (*)(GraphView, BatchArgs, SmemPlan);
 using IntraFn = void (*)(GraphView, BatchArgs, SmemPlan, int);
@@ -1207,6 +1680,25 @@ IntraFn intra_fn_for_nb(uint32_t nb) {
     case 25: return intra_search_kernel<25, RCH>;
     default: return intra_search_kernel<0, RCH>;
   }
+}
+
+using ScatterFn = void (*)(GraphView, BatchArgs, SmemPlan, int, int, uint64_t);
+
+template <int RCH>
+ScatterFn scatter_fn_for_pool(uint32_t pool_cap) {
+  switch (pool_cap) {
+    case 32: return scatter_search_kernel<0, RCH, 1>;
+    case 64: return scatter_search_kernel<0, RCH, 2>;
+    case 128: return scatter_search_kernel<0, RCH, 4>;
+    case 256: return scatter_search_kernel<0, RCH, 8>;
+    default: return scatter_search_kernel<0, RCH, 16>;
+  }
+}
+ScatterFn scatter_fn(const GraphView &g, uint32_t pool_cap) {
+  const uint32_t rch = (g.rstride + 31) / 32;
+  if (rch <= 1) return scatter_fn_for_pool<1>(pool_cap);
+  if (rch <= 2) return scatter_fn_for_pool<2>(pool_cap);
+  return scatter_fn_for_pool<4>(pool_cap);
 }
 
 WarpFn warp_fn(const GraphView &g) {
@@ -1311,6 +1803,39 @@ cudaError_t allow_max_smem(const void *fn) {
   return e;
 }
 }  // namespace
+
+SmemPlan plan_scatter_smem(const GraphView &g, int L_max, int width) {
+  SmemPlan p{};
+  p.q_words = g.nb * 8;
+  p.pool_cap = pow2_at_least(std::max<uint32_t>(32u, (uint32_t)L_max));
+  p.cand_cap = round_up(g.rstride, 32);
+  p.words_per_team = 2 * p.pool_cap + 5 * p.cand_cap;  // per warp
+  p.step_cap = round_up((uint32_t)((sizeof(ScatterCtl) + 3) / 4), 32);
+  uint32_t cap = pow2_at_least(std::max<uint32_t>(2048u, (uint32_t)L_max * (uint32_t)width * 8u));
+  if (cap > 32768) cap = 32768;
+  const uint32_t budget_words = (227u * 1024u) / 4u;
+  const uint32_t fixed = p.q_words + p.step_cap + (uint32_t)width * p.words_per_team;
+  while (cap > 1024 && fixed + cap > budget_words) cap >>= 1;
+  p.hash_cap = cap;
+  p.hash_log2 = log2_of(cap);
+  const uint32_t reserve = (uint32_t)width * p.cand_cap;
+  p.hash_limit = std::min(cap - cap / 4, cap > reserve ? cap - reserve : 0u);
+  return p;
+}
+
+size_t scatter_smem_bytes(const SmemPlan &p, int width) {
+  return (size_t)(p.q_words + p.hash_cap + p.step_cap + (uint32_t)width * p.words_per_team) * 4;
+}
+
+cudaError_t launch_scatter_search(const GraphView &g, const BatchArgs &a, const SmemPlan &p,
+                                  int width, int et, uint64_t seed, cudaStream_t stream) {
+  ScatterFn fn = scatter_fn(g, p.pool_cap);
+  cudaError_t e = allow_max_smem((const void *)fn);
+  if (e != cudaSuccess) return e;
+  if (a.nq == 0) return cudaSuccess;
+  fn<<<a.nq, width * 32, scatter_smem_bytes(p, width), stream>>>(g, a, p, width, et, seed);
+  return cudaGetLastError();
+}
 
 int warp_search_occupancy(const GraphView &g, const SmemPlan &p, int warps_per_block) {
   WarpFn fn = warp_fn(g);

@@ -288,8 +288,12 @@ def test_reference_style_driver_surface(oracle_lib):
     tmp = [0] * 10
     out = idx.SearchArraySimulation(fx["queries"][0], 0, 10, 50, flags, tmp)
     assert tmp == out.tolist() and Flags.resets == 1
-    out2 = idx.MultiThreadSearchArraySimulationWithET(fx["queries"][0], 0, 10, 50, 1, flags, tmp)
-    assert np.array_equal(out, out2)
+    # the intra-query forms are the scatter search: random entry points, so
+    # only the list's shape and the flags reset are fixed
+    out2 = idx.MultiThreadSearchArraySimulationWithET(fx["queries"][0], 0, 10, 50, 4, flags, tmp)
+    assert len(set(out2.tolist())) == 10 and tmp == out2.tolist() and Flags.resets == 2
+    out3 = idx.MultiThreadSearchArraySimulation(fx["queries"][0], 1, 10, 50, 4, flags, tmp)
+    assert len(set(out3.tolist())) == 10 and Flags.resets == 3
     idx.close()
 
 
