@@ -289,7 +289,9 @@ typedef struct ss_server ss_server;
 typedef struct ss_server_config {
   uint32_t max_batch;     /* most requests per launch (1..4096); 0 = 256               */
   uint32_t max_inflight;  /* most launches on the GPU at once (1..16); 0 = 4           */
-  uint32_t max_pending;   /* queued requests before submit says SS_ERR_BUSY; 0 = 1<<16 */
+  uint32_t max_pending;   /* requests held at once (queued, running or finished but not
+                             yet collected by ss_server_wait); beyond it submit says
+                             SS_ERR_BUSY; 0 = 16384                                   */
   int32_t K_max;          /* largest K a request may ask for; 0 = 100                   */
   int32_t L_max;          /* largest L a request may ask for; 0 = 512                   */
   float memory_fraction;  /* share of free device memory the slots may take; 0 = 0.25  */
@@ -307,8 +309,10 @@ typedef struct ss_server_stats {
  * have a graph and outlive the server. */
 int ss_server_create(ss_index *h, const ss_server_config *cfg, ss_server **out);
 
-/* Queues one request (query: dim floats on the host, copied).  Returns
- * SS_ERR_BUSY when max_pending requests are already queued. */
+/* Queues one request (query: dim floats on the host, copied into the
+ * server's preallocated request ring; nothing is allocated per request).
+ * Returns SS_ERR_BUSY when max_pending requests are already held.  Tickets
+ * are nonzero. */
 int ss_server_submit(ss_server *s, const float *query, int K, int L, uint64_t *ticket);
 
 /* Waits up to timeout_ms (< 0: no limit) for a request, copies its K ids and

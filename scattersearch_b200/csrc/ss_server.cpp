@@ -11,6 +11,12 @@
 // free slot, and launches on different slots overlap on the device (each
 // grid is sized to its own batch).  Every query's result is independent of
 // its batch: the kernel keeps no state shared between queries.
+//
+// Requests live in a preallocated ring of max_pending entries indexed by
+// ticket (query, K/L, arrival time, results): tickets are dense and
+// dispatched in order, so the pending ones are exactly [next_dispatch,
+// next_ticket) and submitting allocates nothing.  A ring entry is reused once
+// its ticket has been collected by ss_server_wait.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -18,11 +24,9 @@
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
-#include <deque>
 #include <memory>
 #include <mutex>
 #include <thread>
-#include <unordered_map>
 #include <vector>
 
 #include "scattersearch.h"
@@ -34,13 +38,12 @@ using Clock = std::chrono::steady_clock;
 
 enum ReqState { kPending = 0, kRunning = 1, kDone = 2, kFailed = 3 };
 
+enum : int { kFree = -1 };
+
 struct Request {
-  std::vector<float> q;
   int K = 0, L = 0;
   Clock::time_point t_arrival;
-  int state = kPending;
-  std::vector<uint32_t> ids;
-  std::vector<float> dists;
+  int state = kFree;
   double latency_us = 0.0;
 };
 
@@ -92,11 +95,20 @@ struct ss_server {
 
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
-  std::deque<uint64_t> pending;
-  std::unordered_map<uint64_t, Request> reqs;
-  uint64_t next_ticket = 1;
+  // request ring (max_pending entries), indexed by ticket % cap
+  uint64_t cap = 0;
+  std::vector<Request> ring;
+  std::vector<float> ring_q;      // cap x dim
+  std::vector<uint32_t> ring_ids; // cap x K_max
+  std::vector<float> ring_d;      // cap x K_max
+  uint64_t next_ticket = 0;       // next ticket to hand out
+  uint64_t next_dispatch = 0;     // first ticket not yet launched
+  uint64_t oldest = 0;            // first ticket not yet collected
   bool stop = false;
   std::thread dispatcher;
+
+  Request &req(uint64_t t) { return ring[t % cap]; }
+  uint64_t pending() const { return next_ticket - next_dispatch; }
 
   // statistics
   uint64_t n_submitted = 0, n_completed = 0, n_failed = 0, n_batches = 0, n_batched = 0;
@@ -126,14 +138,14 @@ constexpr size_t kMaxLatencySamples = size_t(1) << 22;
 
 // Copies a finished slot's results to its requests (mu held).
 void ss_server::finish_slot(Slot &sl) {
+  const size_t kx = (size_t)cfg.K_max;
   for (size_t i = 0; i < sl.tickets.size(); ++i) {
-    auto it = reqs.find(sl.tickets[i]);
-    if (it == reqs.end()) continue;
-    Request &r = it->second;
+    const uint64_t t = sl.tickets[i];
+    Request &r = req(t);
     const bool ok = !sl.launch_failed && sl.h_status[i] == ssb::kStatusOk;
     if (ok) {
-      r.ids.assign(sl.h_ids + sl.h_off[i], sl.h_ids + sl.h_off[i] + r.K);
-      r.dists.assign(sl.h_dists + sl.h_off[i], sl.h_dists + sl.h_off[i] + r.K);
+      std::memcpy(&ring_ids[(t % cap) * kx], sl.h_ids + sl.h_off[i], (size_t)r.K * 4);
+      std::memcpy(&ring_d[(t % cap) * kx], sl.h_dists + sl.h_off[i], (size_t)r.K * 4);
     }
     r.latency_us = std::chrono::duration<double, std::micro>(sl.t_done - r.t_arrival).count();
     r.state = ok ? kDone : kFailed;
@@ -143,8 +155,6 @@ void ss_server::finish_slot(Slot &sl) {
     } else {
       ++n_failed;
     }
-    r.q.clear();
-    r.q.shrink_to_fit();
   }
   sl.tickets.clear();
   sl.busy = false;
@@ -156,15 +166,16 @@ void ss_server::finish_slot(Slot &sl) {
 // Launches up to max_batch pending requests on a free slot (mu held on
 // entry and exit).  Returns false if nothing was launched.
 bool ss_server::launch_slot(Slot &sl, std::unique_lock<std::mutex> &lk) {
-  if (pending.empty()) return false;
-  const uint32_t nb = (uint32_t)std::min<size_t>(pending.size(), cfg.max_batch);
-  sl.tickets.assign(pending.begin(), pending.begin() + nb);
-  pending.erase(pending.begin(), pending.begin() + nb);
+  if (pending() == 0) return false;
+  const uint32_t nb = (uint32_t)std::min<uint64_t>(pending(), cfg.max_batch);
+  const uint64_t t0 = next_dispatch;
+  next_dispatch += nb;
+  sl.tickets.resize(nb);
   int64_t off = 0;
   int L_max = 1;
   for (uint32_t i = 0; i < nb; ++i) {
-    Request &r = reqs[sl.tickets[i]];
-    std::memcpy(sl.h_q + (size_t)i * dim, r.q.data(), (size_t)dim * sizeof(float));
+    Request &r = req(t0 + i);
+    sl.tickets[i] = t0 + i;
     sl.h_K[i] = r.K;
     sl.h_L[i] = r.L;
     sl.h_off[i] = off;
@@ -175,6 +186,11 @@ bool ss_server::launch_slot(Slot &sl, std::unique_lock<std::mutex> &lk) {
   sl.busy = true;
   sl.done.store(false, std::memory_order_relaxed);
   lk.unlock();
+  // The ring entries of these tickets stay untouched until they are
+  // collected, so their queries are copied without the lock.
+  for (uint32_t i = 0; i < nb; ++i)
+    std::memcpy(sl.h_q + (size_t)i * dim, &ring_q[((t0 + i) % cap) * dim],
+                (size_t)dim * sizeof(float));
   // Enqueue: inputs up, search, results down, completion callback.
   bool ok = cudaMemcpyAsync(sl.d_q, sl.h_q, (size_t)nb * dim * sizeof(float),
                             cudaMemcpyHostToDevice, sl.stream) == cudaSuccess &&
@@ -222,7 +238,7 @@ void ss_server::run() {
     cv_work.wait(lk, [&] {
       for (auto &sl : slots) {
         if (sl->busy && sl->done.load(std::memory_order_acquire)) return true;
-        if (!sl->busy && !pending.empty() && !stop) return true;
+        if (!sl->busy && pending() > 0 && !stop) return true;
       }
       if (stop) {
         for (auto &sl : slots)
@@ -240,21 +256,20 @@ int ss_server::submit_at(const float *query, int K, int L, Clock::time_point t_a
   if (K < 1 || K > L || K > cfg.K_max || L > cfg.L_max)
     return ssb::index_error(h, SS_ERR_INVALID_ARGUMENT,
                             "request needs 1 <= K <= L, K <= K_max and L <= L_max");
-  Request r;
-  r.q.assign(query, query + dim);
-  r.K = K;
-  r.L = L;
-  r.t_arrival = t_arrival;
   {
     std::lock_guard<std::mutex> lk(mu);
     if (stop) return ssb::index_error(h, SS_ERR_INVALID_ARGUMENT, "server is stopping");
-    if (pending.size() >= cfg.max_pending)
+    if (next_ticket - oldest >= cap)
       return ssb::index_error(h, SS_ERR_BUSY, "request queue is full");
     const uint64_t t = next_ticket++;
-    reqs.emplace(t, std::move(r));
-    pending.push_back(t);
+    Request &r = req(t);
+    std::memcpy(&ring_q[(t % cap) * dim], query, (size_t)dim * sizeof(float));
+    r.K = K;
+    r.L = L;
+    r.t_arrival = t_arrival;
+    r.state = kPending;
     ++n_submitted;
-    *ticket = t;
+    *ticket = t + 1;  // tickets handed out start at 1
   }
   cv_work.notify_all();
   return SS_OK;
@@ -295,11 +310,12 @@ int ss_server_create(ss_index *h, const ss_server_config *cfg, ss_server **out) 
   if (cfg) c = *cfg;
   if (c.max_batch == 0) c.max_batch = 256;
   if (c.max_inflight == 0) c.max_inflight = 4;
-  if (c.max_pending == 0) c.max_pending = 1u << 16;
+  if (c.max_pending == 0) c.max_pending = 1u << 14;
   if (c.K_max == 0) c.K_max = 100;
   if (c.L_max == 0) c.L_max = 512;
   if (c.memory_fraction <= 0.f) c.memory_fraction = 0.25f;
-  if (c.max_batch > 4096 || c.max_inflight > 16 || c.K_max < 1 || c.L_max < c.K_max ||
+  if (c.max_batch > 4096 || c.max_inflight > 16 || c.max_pending > (1u << 24) || c.K_max < 1 ||
+      c.L_max < c.K_max ||
       c.L_max > SS_MAX_L || c.memory_fraction > 1.f)
     return ssb::index_error(h, SS_ERR_INVALID_ARGUMENT, "server configuration out of range");
 
@@ -308,6 +324,12 @@ int ss_server_create(ss_index *h, const ss_server_config *cfg, ss_server **out) 
   s->device = ssb::index_device(h);
   s->dim = ssb::index_dim(h);
   s->cfg = c;
+  s->cap = c.max_pending;
+  s->ring.resize(s->cap);
+  s->ring_q.resize((size_t)s->cap * s->dim);
+  s->ring_ids.resize((size_t)s->cap * (size_t)c.K_max);
+  s->ring_d.resize((size_t)s->cap * (size_t)c.K_max);
+  s->latencies.reserve(kMaxLatencySamples);
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(s->device);
@@ -365,20 +387,23 @@ int ss_server_wait(ss_server *s, uint64_t ticket, int timeout_ms, uint32_t *ids,
                    double *latency_us) {
   if (!s) return ssb::index_error(nullptr, SS_ERR_INVALID_ARGUMENT, "null server");
   std::unique_lock<std::mutex> lk(s->mu);
-  auto it = s->reqs.find(ticket);
-  if (it == s->reqs.end()) return ssb::index_error(s->h, SS_ERR_INVALID_ARGUMENT, "unknown ticket");
-  auto ready = [&] { return it->second.state >= kDone; };
+  const uint64_t t = ticket - 1;
+  if (ticket == 0 || t < s->oldest || t >= s->next_ticket || s->req(t).state == kFree)
+    return ssb::index_error(s->h, SS_ERR_INVALID_ARGUMENT, "unknown ticket");
+  Request &r = s->req(t);
+  auto ready = [&] { return r.state >= kDone; };
   if (timeout_ms < 0) {
     s->cv_done.wait(lk, ready);
   } else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) {
     return ssb::index_error(s->h, SS_ERR_TIMEOUT, "request not finished within the timeout");
   }
-  Request &r = it->second;
   const bool ok = r.state == kDone;
-  if (ok && ids) std::memcpy(ids, r.ids.data(), (size_t)r.K * sizeof(uint32_t));
-  if (ok && dists) std::memcpy(dists, r.dists.data(), (size_t)r.K * sizeof(float));
+  const size_t kx = (size_t)s->cfg.K_max;
+  if (ok && ids) std::memcpy(ids, &s->ring_ids[(t % s->cap) * kx], (size_t)r.K * sizeof(uint32_t));
+  if (ok && dists) std::memcpy(dists, &s->ring_d[(t % s->cap) * kx], (size_t)r.K * sizeof(float));
   if (latency_us) *latency_us = r.latency_us;
-  s->reqs.erase(it);
+  r.state = kFree;
+  while (s->oldest < s->next_ticket && s->req(s->oldest).state == kFree) ++s->oldest;
   if (!ok) return ssb::index_error(s->h, SS_ERR_SEARCH_LIMIT, "request failed on the device");
   return SS_OK;
 }
@@ -461,11 +486,8 @@ void ss_server_destroy(ss_server *s) {
   {
     std::lock_guard<std::mutex> lk(s->mu);
     s->stop = true;
-    for (uint64_t t : s->pending) {
-      auto it = s->reqs.find(t);
-      if (it != s->reqs.end()) it->second.state = kFailed;
-    }
-    s->pending.clear();
+    for (uint64_t t = s->next_dispatch; t < s->next_ticket; ++t) s->req(t).state = kFailed;
+    s->next_dispatch = s->next_ticket;
   }
   s->cv_work.notify_all();
   s->cv_done.notify_all();

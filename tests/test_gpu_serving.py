@@ -93,3 +93,30 @@ def test_concurrent_submitters():
         with pytest.raises(SearchError):
             srv.submit(Q[0], 5, 65)
     idx.close()
+
+
+def test_request_ring_fills_and_wraps():
+    from scattersearch_b200 import SearchError
+    from scattersearch_b200.serving import Server
+    fx = load_fixture("search_ip_d96")
+    idx = _index(fx)
+    Q = fx["queries"]
+    alone = _alone(idx, Q, [10] * len(Q), [40] * len(Q))
+    with Server(idx, max_batch=4, max_inflight=2, max_pending=8, K_max=10, L_max=40) as srv:
+        tickets = [srv.submit(Q[i], 10, 40) for i in range(8)]
+        with pytest.raises(SearchError) as e:
+            srv.submit(Q[8], 10, 40)  # eight requests held, none collected
+        assert e.value.code == 9  # SS_ERR_BUSY
+        for i, t in enumerate(tickets):
+            ids, d, _ = srv.wait(t, 10)
+            assert np.array_equal(ids, alone[i][0]) and _same(d, alone[i][1])
+        with pytest.raises(SearchError):
+            srv.wait(tickets[0], 10)  # already collected
+        # many wraps of the 8-entry ring, results still per query
+        for rnd in range(5):
+            part = list(range(rnd * 8, rnd * 8 + 8))
+            tk = [(i % len(Q), srv.submit(Q[i % len(Q)], 10, 40)) for i in part]
+            for i, t in tk:
+                ids, d, _ = srv.wait(t, 10)
+                assert np.array_equal(ids, alone[i][0]) and _same(d, alone[i][1]), (rnd, i)
+    idx.close()
