@@ -51,6 +51,8 @@ struct SmemPlan {
   uint32_t step_cap;    // CTA kernel: step-local dedupe table (power of two)
   uint32_t step_log2;
   uint32_t stage_rows;  // warp kernel: rows of the shared-memory row stage
+  uint32_t stage_split; // warp kernel: 1 = whole rows, 2 = rows staged in two halves
+  uint32_t stage_row_words;  // warp kernel: floats per staged row
   uint32_t stage_words; // warp kernel: size of the row stage
   uint32_t words_per_team;
 };

@@ -323,11 +323,33 @@ struct RowStage {
   bool broken;      // a wait timed out: the stage may still be written to
 };
 
-// Starts copying the base rows of cid[0..m) (m <= the stage's rows) into the
-// stage.  All 32 lanes call it; cid must be visible to every lane.
+// Blocks (8 floats each) of the first half-row of a split stage: the odd
+// tail block (processed first, distance.cpp:42-45) plus the leading blocks.
+__host__ __device__ __forceinline__ uint32_t split_first(uint32_t nb) { return (nb + 1) / 2; }
+
+// Starts copying part `part` of the base rows of cid[0..m) (m <= the stage's
+// rows) into the stage: part 2 is the whole row (memory order); with a split
+// stage, part 0 is the first half of the blocks in processing order (the odd
+// tail block, then blocks 0, 1, ...) and part 1 the rest.  All 32 lanes call
+// it; cid must be visible to every lane.
 __device__ __forceinline__ void stage_issue(const GraphView &g, const WarpSmem &s, const RowStage &st,
-                                            const uint32_t *cid, int m, int lane) {
-  const uint32_t bytes = g.nb * 32u;
+                                            const uint32_t *cid, int m, int part, uint32_t row_words,
+                                            int lane) {
+  const uint32_t nb = g.nb, A = split_first(nb);
+  const bool odd = nb & 1u;
+  uint32_t bytes, src_block, dst_block = 0, nblocks;
+  if (part == 2) {
+    nblocks = nb;
+    src_block = 0;
+  } else if (part == 0) {
+    nblocks = odd ? A - 1 : A;
+    src_block = 0;
+    dst_block = odd ? 1 : 0;
+  } else {
+    nblocks = nb - A;
+    src_block = odd ? A - 1 : A;
+  }
+  bytes = (nblocks + (part == 0 && odd ? 1u : 0u)) * 32u;
   // earlier reads of the stage (generic proxy) come before the copies that
   // overwrite it (async proxy)
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -337,12 +359,20 @@ __device__ __forceinline__ void stage_issue(const GraphView &g, const WarpSmem &
                  : "memory");
   __syncwarp();
   if (lane < m) {
-    const float *src = g.base + (size_t)cid[lane] * (size_t)(g.nb * 8);
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_addr(s.stage + lane * (g.nb * 8))),
-        "l"(src), "r"(bytes), "r"(st.bar)
-        : "memory");
+    const float *row = g.base + (size_t)cid[lane] * (size_t)(nb * 8);
+    float *dst = s.stage + lane * row_words;
+    if (nblocks > 0)
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+              smem_addr(dst + dst_block * 8)),
+          "l"(row + src_block * 8), "r"(nblocks * 32u), "r"(st.bar)
+          : "memory");
+    if (part == 0 && odd)
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+              smem_addr(dst)),
+          "l"(row + (nb - 1) * 8), "r"(32u), "r"(st.bar)
+          : "memory");
   }
 }
 
@@ -354,39 +384,43 @@ __device__ __forceinline__ bool stage_wait(RowStage &st) {
   return __all_sync(kFull, ok);
 }
 
-// Distance between the query and staged row `c`, computed by a lane pair:
-// lane h (0/1) of the pair owns reference lanes 4h..4h+3 (the arithmetic of
-// pair_distance, with both operands in shared memory).
-template <int NB>
-__device__ __forceinline__ float staged_distance(const GraphView &g, const float *qs,
-                                                 const float *row, int h) {
+// Lane-pair accumulation over processing steps [T0, T1) of the reference
+// model (step t = block block_at(t, nb)) from a staged row: lane h (0/1) of
+// the pair owns reference lanes 4h..4h+3.  WHOLE: the staged row is in
+// memory order (block b at b); otherwise the staged part holds steps
+// T0..T1-1 in order.
+template <int NB, bool WHOLE>
+__device__ __forceinline__ void staged_accumulate(const GraphView &g, const float *qs,
+                                                  const float *row, int h, int T0, int T1,
+                                                  float &a0, float &a1, float &a2, float &a3) {
   const int nb = NB > 0 ? NB : (int)g.nb;
   const float4 *r4 = reinterpret_cast<const float4 *>(row) + h;
   const float4 *q4 = reinterpret_cast<const float4 *>(qs) + h;
-  float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
   const bool l2 = g.metric == 0;
   if constexpr (NB > 0) {
-    if (l2) {
 #pragma unroll
-      for (int t = 0; t < NB; ++t) {
-        const int b = block_at(t, NB);
-        acc_l2(a0, a1, a2, a3, q4[2 * b], r4[2 * b]);
-      }
-    } else {
-#pragma unroll
-      for (int t = 0; t < NB; ++t) {
-        const int b = block_at(t, NB);
-        acc_ip(a0, a1, a2, a3, q4[2 * b], r4[2 * b]);
-      }
+    for (int t = 0; t < NB; ++t) {
+      if (t < T0 || t >= T1) continue;
+      const int b = block_at(t, NB);
+      const int sb = WHOLE ? b : t - T0;
+      if (l2) acc_l2(a0, a1, a2, a3, q4[2 * b], r4[2 * sb]);
+      else acc_ip(a0, a1, a2, a3, q4[2 * b], r4[2 * sb]);
     }
   } else {
 #pragma unroll 4
-    for (int t = 0; t < nb; ++t) {
+    for (int t = T0; t < T1; ++t) {
       const int b = block_at(t, nb);
-      if (l2) acc_l2(a0, a1, a2, a3, q4[2 * b], r4[2 * b]);
-      else acc_ip(a0, a1, a2, a3, q4[2 * b], r4[2 * b]);
+      const int sb = WHOLE ? b : t - T0;
+      if (l2) acc_l2(a0, a1, a2, a3, q4[2 * b], r4[2 * sb]);
+      else acc_ip(a0, a1, a2, a3, q4[2 * b], r4[2 * sb]);
     }
   }
+}
+
+// Horizontal sum u0 + u1 + ... + u7 of a lane pair's partials, left to right
+// (distance.cpp:53); both lanes return the distance.
+__device__ __forceinline__ float pair_finish(const GraphView &g, int h, float a0, float a1, float a2,
+                                             float a3) {
   const float o0 = __shfl_xor_sync(kFull, a0, 1);
   const float o1 = __shfl_xor_sync(kFull, a1, 1);
   const float o2 = __shfl_xor_sync(kFull, a2, 1);
@@ -400,24 +434,45 @@ __device__ __forceinline__ float staged_distance(const GraphView &g, const float
   r = __fadd_rn(r, u1);
   r = __fadd_rn(r, u2);
   r = __fadd_rn(r, u3);
-  return l2 ? r : -r;
+  return g.metric == 0 ? r : -r;
 }
 
-// Keys of cid[0..nc) into ckey[0..nc): rows beyond the first stage load are
-// sent to L2 first, then stage loads of `srows` rows (<= 16), one distance
-// per lane pair.  When `first_issued`, the first load was already started
-// with stage_issue.  Returns false when a stage wait timed out.
+// Keys of cid[0..nc) into ckey[0..nc) in passes of `srows` rows (<= 16),
+// one distance per lane pair.  With a whole-row stage, rows beyond the first
+// pass are sent to L2 first; with a split stage every row is, and each pass
+// loads the first halves, accumulates, then loads the second halves (L2
+// hits) into the same buffer.  When `first_issued`, the first load (part 0,
+// or the whole rows) was already started with stage_issue.  Returns false
+// when a stage wait timed out.
 template <int NB>
 __device__ __forceinline__ bool eval_staged(const GraphView &g, const WarpSmem &s, RowStage &st,
-                                            const uint32_t *cid, uint32_t *ckey, int nc, int srows,
-                                            bool first_issued, int lane) {
-  if (nc > srows) prefetch_rows(g, cid + srows, nc - srows, lane);
+                                            const SmemPlan &p, const uint32_t *cid, uint32_t *ckey,
+                                            int nc, bool first_issued, int lane) {
+  const int srows = (int)p.stage_rows;
+  const bool split = p.stage_split > 1;
+  const int nb = NB > 0 ? NB : (int)g.nb;
+  const int A = (int)split_first((uint32_t)nb);
+  if (split) prefetch_rows(g, cid, nc, lane);
+  else if (nc > srows) prefetch_rows(g, cid + srows, nc - srows, lane);
   const int h = lane & 1, c = lane >> 1;
   for (int p0 = 0; p0 < nc; p0 += srows) {
     const int m = min(srows, nc - p0);
-    if (p0 > 0 || !first_issued) stage_issue(g, s, st, cid + p0, m, lane);
-    if (!stage_wait(st)) return false;
-    const float d = staged_distance<NB>(g, s.q, s.stage + (c < m ? c : 0) * (g.nb * 8), h);
+    const float *row = s.stage + (c < m ? c : 0) * p.stage_row_words;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+    if (!split) {
+      if (p0 > 0 || !first_issued) stage_issue(g, s, st, cid + p0, m, 2, p.stage_row_words, lane);
+      if (!stage_wait(st)) return false;
+      staged_accumulate<NB, true>(g, s.q, row, h, 0, nb, a0, a1, a2, a3);
+    } else {
+      if (p0 > 0 || !first_issued) stage_issue(g, s, st, cid + p0, m, 0, p.stage_row_words, lane);
+      if (!stage_wait(st)) return false;
+      staged_accumulate<NB, false>(g, s.q, row, h, 0, A, a0, a1, a2, a3);
+      __syncwarp();
+      stage_issue(g, s, st, cid + p0, m, 1, p.stage_row_words, lane);
+      if (!stage_wait(st)) return false;
+      staged_accumulate<NB, false>(g, s.q, row, h, A, nb, a0, a1, a2, a3);
+    }
+    const float d = pair_finish(g, h, a0, a1, a2, a3);
     if (h == 0 && c < m) ckey[p0 + c] = float_to_key(d);
     __syncwarp();
   }
@@ -629,7 +684,7 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
       size += __popc(__ballot_sync(kFull, valid));
     }
     __syncwarp();
-    if (!eval_staged<NB>(g, s, st, s.cid, s.ckey, size, (int)p.stage_rows, false, lane)) {
+    if (!eval_staged<NB>(g, s, st, p, s.cid, s.ckey, size, false, lane)) {
       status = kStatusStageTimeout;
       size = 0;
     }
@@ -718,7 +773,8 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
       nc += __popc(fm);
       if (RCH == 1 && nc > 0) {
         __syncwarp();
-        stage_issue(g, s, st, s.cid, min(nc, srows), lane);
+        stage_issue(g, s, st, s.cid, min(nc, srows), p.stage_split > 1 ? 0 : 2,
+                    p.stage_row_words, lane);
         issued = true;
       }
       qh_record(vis, pr, row[c], fresh, lane);
@@ -733,7 +789,7 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
     __syncwarp();
 
     // 3. distances of the staged rows
-    if (!eval_staged<NB>(g, s, st, s.cid, s.ckey, nc, srows, issued, lane)) {
+    if (!eval_staged<NB>(g, s, st, p, s.cid, s.ckey, nc, issued, lane)) {
       status = kStatusStageTimeout;
       break;
     }
@@ -1751,10 +1807,16 @@ SmemPlan plan_warp_smem(const GraphView &g, int L_max, int hash_cap_override) {
   p.qh_rbits = nbits > bbits ? nbits - bbits : 0;
   p.hash_cap = (1u << bbits) * 8;
   p.hash_limit = p.hash_cap;
-  // row stage: 16 rows, fewer for rows so wide that 16 would pass 64 KB
+  // Row stage: 16 whole rows.  Rows so wide that 16 of them would pass 64 KB
+  // (over 4 KB each) are staged in two halves, keeping 16 rows per pass at
+  // the cost of one L2 round trip per pass (measured slower than whole rows
+  // at 200 dims: 546k against 640k queries/s at L = 400), and fewer rows
+  // only beyond that.
+  p.stage_split = kStageRows * g.nb * 32u > 65536u ? 2 : 1;
+  p.stage_row_words = (p.stage_split > 1 ? split_first(g.nb) : g.nb) * 8;
   p.stage_rows = kStageRows;
-  while (p.stage_rows > 1 && p.stage_rows * g.nb * 32u > 65536u) p.stage_rows >>= 1;
-  p.stage_words = p.stage_rows * g.nb * 8;
+  while (p.stage_rows > 1 && p.stage_rows * p.stage_row_words * 4u > 65536u) p.stage_rows >>= 1;
+  p.stage_words = p.stage_rows * p.stage_row_words;
   p.words_per_team = p.stage_words + 4 + p.q_words + 2 * p.pool_cap + 5 * p.cand_cap +
                      (1u << bbits) * 4;
   p.words_per_team = round_up(p.words_per_team, 32);  // 128-byte aligned stages

@@ -121,10 +121,11 @@ def _synthetic(seed, n, dim, R, metric, clusters=8):
 
 
 @pytest.mark.parametrize("dim,R,metric", [(128, 64, 0), (96, 32, 1), (13, 16, 0), (200, 32, 1),
-                                          (256, 100, 0)])
+                                          (256, 100, 0), (1100, 16, 0), (1100, 16, 1)])
 def test_synthetic_shapes(oracle_lib, dim, R, metric):
-    """Generic dims (13 is not a multiple of 8, 256 has no specialisation)
-    and wide graphs (R = 64 and 100 take two and four 32-id chunks)."""
+    """Generic dims (13 is not a multiple of 8, 256 has no specialisation,
+    1100 rows are staged in two halves), and wide graphs (R = 64 and 100
+    take two and four 32-id chunks)."""
     O = oracle_lib
     X, Q, adj, ep = _synthetic(dim + R, 4000, dim, R, metric)
     idx = _index(X, adj, ep, metric)
