@@ -155,6 +155,11 @@ int ss_search_batch_device(ss_index *h, const float *queries, uint32_t nq, const
 typedef struct ss_plan ss_plan;
 int ss_plan_create(ss_index *h, const float *queries, uint32_t nq, int K, int L, uint32_t *ids,
                    float *dists, ss_plan **out);
+/* Same for a batch with per-query K and L: Ks, Ls and out_off are device
+ * arrays of nq entries, as for ss_search_batch_device; L_max bounds Ls. */
+int ss_plan_create_uneven(ss_index *h, const float *queries, uint32_t nq, const int32_t *Ks,
+                          const int32_t *Ls, const int64_t *out_off, int K, int L, int L_max,
+                          uint32_t *ids, float *dists, ss_plan **out);
 int ss_plan_launch(ss_plan *p, void *stream);
 int ss_plan_status(ss_plan *p, uint32_t *failed_queries);
 void ss_plan_destroy(ss_plan *p);

@@ -49,6 +49,8 @@ SIGNATURES = {
                                       _vp, _vp, _vp]),
     "ss_batch_status": (_i32, [_vp, _u32p]),
     "ss_plan_create": (_i32, [_vp, _vp, _u32, _i32, _i32, _vp, _vp, _hp]),
+    "ss_plan_create_uneven": (_i32, [_vp, _vp, _u32, _vp, _vp, _vp, _i32, _i32, _i32, _vp, _vp,
+                                     _hp]),
     "ss_plan_launch": (_i32, [_vp, _vp]),
     "ss_plan_status": (_i32, [_vp, _u32p]),
     "ss_plan_destroy": (None, [_vp]),

@@ -318,6 +318,16 @@ class ANNSearch:
                                              _dptr(ids), _dptr(dists), ctypes.byref(p)))
         return SearchPlan(self, p)
 
+    def plan_batch_uneven_device(self, queries, nq: int, Ks, Ls, out_off, L_max: int, ids,
+                                 dists=None):
+        """Graph-captured batched search with per-query K/L (device arrays
+        Ks, Ls, out_off); returns a ``SearchPlan``."""
+        p = ctypes.c_void_p()
+        self._check(self._lib.ss_plan_create_uneven(
+            self._h, _dptr(queries), int(nq), _dptr(Ks), _dptr(Ls), _dptr(out_off), 0, 0,
+            int(L_max), _dptr(ids), _dptr(dists), ctypes.byref(p)))
+        return SearchPlan(self, p)
+
     def batch_status(self) -> int:
         """Failed queries of the last device batch (call after synchronising)."""
         n = ctypes.c_uint32()

@@ -751,10 +751,20 @@ extern "C" {
 
 int ss_plan_create(ss_index *h, const float *queries, uint32_t nq, int K, int L, uint32_t *ids,
                    float *dists, ss_plan **out) {
+  return ss_plan_create_uneven(h, queries, nq, nullptr, nullptr, nullptr, K, L, L, ids, dists, out);
+}
+
+int ss_plan_create_uneven(ss_index *h, const float *queries, uint32_t nq, const int32_t *Ks,
+                          const int32_t *Ls, const int64_t *out_off, int K, int L, int L_max,
+                          uint32_t *ids, float *dists, ss_plan **out) {
   if (!out) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null output plan");
   *out = nullptr;
-  int rc = check_search_args(h, K, L);
+  const bool uneven = Ks != nullptr;
+  if (uneven != (Ls != nullptr) || uneven != (out_off != nullptr))
+    return set_err(h, SS_ERR_INVALID_ARGUMENT, "Ks, Ls and out_off must be given together");
+  int rc = uneven ? check_search_args(h, 1, L_max) : check_search_args(h, K, L);
   if (rc) return rc;
+  if (!uneven) L_max = L;
   if (nq == 0 || !queries || !ids)
     return set_err(h, SS_ERR_INVALID_ARGUMENT, "a plan needs nq > 0, queries and ids");
   DeviceGuard dg(h->device);
@@ -774,18 +784,21 @@ int ss_plan_create(ss_index *h, const float *queries, uint32_t nq, int K, int L,
   // Plan the launch outside the capture (occupancy queries and kernel
   // attributes are not stream work).
   ssb::GraphView g = h->view();
-  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L, h->hash_cap_override);
+  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, h->hash_cap_override);
   const int wpb = choose_wpb(h, plan);
   const int blocks = persistent_blocks(h, plan, wpb, nq);
   if ((size_t)plan.words_per_team * 4 * wpb > 227 * 1024 || blocks <= 0) {
     plan_free(p);
     cudaStreamDestroy(cs);
-    return set_err(h, SS_ERR_UNSUPPORTED, "L=%d cannot be planned on this device", L);
+    return set_err(h, SS_ERR_UNSUPPORTED, "L=%d cannot be planned on this device", L_max);
   }
   ssb::BatchArgs a{};
   a.queries = queries;
   a.qstride = h->dim;
   a.nq = nq;
+  a.Ks = Ks;
+  a.Ls = Ls;
+  a.out_off = out_off;
   a.K0 = K;
   a.L0 = L;
   a.ids = ids;

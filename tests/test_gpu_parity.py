@@ -338,3 +338,31 @@ def test_autotuner_keeps_results_and_caches_its_choice(oracle_lib, tmp_path):
     idx.set_tuning()
     assert autotune.apply(idx, 100, path=path)["hash_cap"] == choice["hash_cap"]
     idx.close()
+
+
+def test_graph_captured_uneven_plan(oracle_lib):
+    import torch
+    fx = load_fixture("search_l2_d200")
+    idx = _index(fx["base"], fx["adj"], fx["ep"], 0)
+    rng = np.random.default_rng(23)
+    Q = fx["queries"]
+    nq = len(Q)
+    Ks = rng.choice(np.array([1, 10, 100], np.int32), nq)
+    Ls = np.maximum(Ks, rng.integers(32, 513, nq)).astype(np.int32)
+    off = np.concatenate([[0], np.cumsum(Ks)[:-1]]).astype(np.int64)
+    total = int(Ks.sum())
+    q = torch.as_tensor(Q).cuda()
+    dK, dL, doff = (torch.as_tensor(x).cuda() for x in (Ks, Ls, off))
+    ids = torch.empty(total, dtype=torch.int32, device="cuda")
+    d = torch.empty(total, dtype=torch.float32, device="cuda")
+    plan = idx.plan_batch_uneven_device(q, nq, dK, dL, doff, 512, ids, d)
+    o_ids, o_d, _, _ = oracle_lib.search(fx["base"], fx["adj"], int(fx["ep"]), 0, Q, Ks=Ks, Ls=Ls)
+    s = torch.cuda.current_stream()
+    for _ in range(2):
+        plan.launch(s.cuda_stream)
+        s.synchronize()
+        assert plan.failed_queries() == 0
+        assert np.array_equal(ids.cpu().numpy().view(np.uint32), o_ids)
+        assert _same_bits(d.cpu().numpy(), o_d)
+    plan.close()
+    idx.close()
