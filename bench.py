@@ -77,16 +77,20 @@ def parse_args(argv=None):
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="cfg3", choices=["cfg1", "cfg2", "cfg3"])
+    ap.add_argument("--workload", default="cfg3", choices=["cfg1", "cfg2", "cfg3", "cfg4"])
     ap.add_argument("--L", default="auto")
-    ap.add_argument("--nq", type=int, default=10000, help="queries per GPU")
+    ap.add_argument("--nq", type=int, default=None,
+                    help="queries per GPU (default 10000; 100000 for cfg4)")
     ap.add_argument("--scale", type=float, default=1.0, help="base size fraction (profiling)")
     ap.add_argument("--plain-sample", type=int, default=300)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-online", action="store_true",
                     help="skip the serving and intra-query latency legs")
-    return ap.parse_args(argv)
+    args = ap.parse_args(argv)
+    if args.nq is None:
+        args.nq = 100_000 if args.workload == "cfg4" else 10_000
+    return args
 
 
 # --------------------------------------------------------------- plumbing
@@ -198,6 +202,9 @@ def measured_hbm_peak():
 
 # --------------------------------------------------------------- workload
 def workload_spec(name):
+    if name == "cfg4":
+        return dict(cfg=4, Ls=[], K=100, desc="5Mx96 angular (IP), per-query K in {1,10,100} "
+                                               "and L in [32,512]", gt_sample=10000)
     if name == "cfg3":
         return dict(cfg=3, Ls=[200, 400, 800], K=100, desc="1.2Mx200 angular (IP), K=100")
     if name == "cfg2":
@@ -216,13 +223,17 @@ def build_workload(args, rank, world, device):
     log(f"data {w.base.shape} queries {queries.shape} in {time.time() - t0:.1f}s")
     t0 = time.time()
     X = torch.from_numpy(w.base).to(device)
-    adj, ep = graph.build_graph(X, R=w.graph_R, knn_k=w.graph_knn, device=device)
+    # large bases: bigger k-NN distance blocks (fewer launches), within HBM
+    budget = 24e9 if X.shape[0] > 2_000_000 and device != "cpu" else 6e9
+    adj, ep = graph.build_graph(X, R=w.graph_R, knn_k=w.graph_knn, device=device,
+                                knn_budget_bytes=budget)
     log(f"graph R={w.graph_R} ep={ep} mean degree {(adj != 0xFFFFFFFF).sum(1).mean():.1f} "
         f"in {time.time() - t0:.1f}s")
     Q = torch.from_numpy(queries).to(device)
     if device != "cpu" and torch.cuda.is_available():
         torch.cuda.empty_cache()  # hand the graph build's scratch back to the driver
-    gt, gt_info = ground_truth(X, Q, w.metric, device)
+    ns = min(len(queries), spec.get("gt_sample", len(queries)))
+    gt, gt_info = ground_truth(X, Q[:ns], w.metric, device)
     log(f"ground truth: {gt_info}")
     return dict(spec=spec, w=w, X=X, queries=queries, Q=Q, adj=adj, ep=ep,
                 gt=gt, gt_info=gt_info, metric=w.metric, K=spec["K"])
@@ -316,6 +327,10 @@ def _reference_arm(args):
         return None
     import torch
     from oracle import oracle as O
+    if args.workload == "cfg4":
+        d.close()
+        return {"impl": "reference", "unavailable": "the reference's drivers take one K and L "
+                "per run; per-query K/L batches have no reference entry point"}
     if not O.have_reference(fast=True):
         d.close()
         return {"impl": "reference", "unavailable": "oracle/_ref/libssref_fast.so was not built"}
@@ -670,11 +685,205 @@ def run_ours(args):
     d.close()
     return 0
 
+def recall_uneven(ids_flat, off, Ks, gt):
+    """recall@10 over the sampled queries with K >= 10 and recall@1 over those
+    with K = 1 (query i's list starts at off[i])."""
+    r10, r1 = [], []
+    for i in range(len(gt)):
+        k = int(Ks[i])
+        got = ids_flat[off[i]:off[i] + min(k, 10)].astype(np.int64)
+        if k >= 10:
+            r10.append(np.isin(got, gt[i]).sum() / 10.0)
+        else:
+            r1.append(float(got[0] == gt[i][0]))
+    return (float(np.mean(r10)) if r10 else None, float(np.mean(r1)) if r1 else None,
+            len(r10), len(r1))
+
+
+def run_uneven(args):
+    """Config 4: one batch with per-query K and L, searched by one persistent
+    launch captured in a CUDA graph (ss_plan_create_uneven)."""
+    import torch
+    d = Dist("nccl")
+    torch.cuda.set_device(d.local_rank)
+    device = torch.device("cuda", d.local_rank)
+    from scattersearch_b200 import ANNSearch, autotune, datasets
+    wl = build_workload(args, d.rank, d.world, device)
+    nq, dim = wl["queries"].shape
+    Ks, Ls = datasets.uneven_k_l(nq * d.world)
+    Ks = np.ascontiguousarray(Ks[d.rank * nq:(d.rank + 1) * nq])
+    Ls = np.ascontiguousarray(Ls[d.rank * nq:(d.rank + 1) * nq])
+    off = np.concatenate([[0], np.cumsum(Ks.astype(np.int64))[:-1]]).astype(np.int64)
+    total = int(Ks.sum())
+    L_max = int(Ls.max())
+    idx = ANNSearch(dim, wl["X"].shape[0], wl["X"], wl["metric"], base_on_device=True)
+    idx.SetGraph(wl["adj"], wl["ep"])
+    Qd = wl["Q"]
+    dK, dL, doff = (torch.from_numpy(a).to(device) for a in (Ks, Ls, off))
+    tune = autotune.autotune(idx, Qd, total, L_max, reps=2, path=None, Ks=dK, Ls=dL,
+                             out_off=doff)
+    log(f"tuned: {tune['warps_per_block']} teams per CTA, {tune['hash_cap']}-slot visited table")
+    ids_d = torch.empty(total, dtype=torch.int32, device=device)
+    dist_d = torch.empty(total, dtype=torch.float32, device=device)
+    ndc_d = torch.empty(nq, dtype=torch.int32, device=device)
+    hops_d = torch.empty(nq, dtype=torch.int32, device=device)
+    stream = torch.cuda.current_stream()
+
+    def stats_pass():
+        idx.search_batch_device(Qd, nq, ids_d, dist_d, Ks=dK, Ls=dL, out_off=doff, L_max=L_max,
+                                ndc=ndc_d, hops=hops_d, stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        if idx.batch_status():
+            raise RuntimeError("device batch reported failed queries")
+
+    idx.set_tuning(hash_cap=65536)  # exact distance-evaluation counts
+    stats_pass()
+    ndc = ndc_d.cpu().numpy().astype(np.int64)
+    hops = hops_d.cpu().numpy().astype(np.int64)
+    ids_exact = ids_d.cpu().numpy().copy()
+    idx.set_tuning(tune["warps_per_block"], tune["hash_cap"], 0)
+    stats_pass()
+    ndc_dev = ndc_d.cpu().numpy().astype(np.int64)
+    if not np.array_equal(ids_d.cpu().numpy(), ids_exact):
+        raise RuntimeError("ids depend on the visited-table size")
+    plan = idx.plan_batch_uneven_device(Qd, nq, dK, dL, doff, L_max, ids_d, dist_d)
+    rstride = idx.rstride
+    bytes_per_step = float(ndc.sum() * 4 * dim + hops.sum() * 4 * rstride + nq * 4 * dim)
+
+    for _ in range(args.warmup):
+        plan.launch(stream.cuda_stream)
+    torch.cuda.synchronize()
+    d.barrier()
+    sampler = ClockSampler(d.local_rank)
+    sampler.start()
+    evs = []
+    for _ in range(args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        plan.launch(stream.cuda_stream)
+        b.record(stream)
+        evs.append((a, b))
+    torch.cuda.synchronize()
+    d.barrier()
+    clocks = sampler.stop()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    if plan.failed_queries():
+        raise RuntimeError("graph-captured search reported failed queries")
+    total_s = d.max(sum(step_ms) / 1000.0, device)
+    qps = nq * d.world * args.steps / total_s
+    ids_np = ids_d.cpu().numpy().view(np.uint32)
+    if not np.array_equal(ids_np, ids_exact.view(np.uint32)):
+        raise RuntimeError("graph replay returned other ids than the direct launch")
+    r10, r1, n10, n1 = recall_uneven(ids_np, off, Ks, wl["gt"])
+
+    # e2e: public C ABI (ss_search_batch_uneven) with pinned host buffers
+    qh = torch.empty((nq, dim), dtype=torch.float32).pin_memory()
+    qh.numpy()[:] = wl["queries"]
+    ih = torch.empty(total, dtype=torch.int32).pin_memory()
+    dh = torch.empty(total, dtype=torch.float32).pin_memory()
+    qn, idn, dn = qh.numpy(), ih.numpy().view(np.uint32), dh.numpy()
+    for _ in range(max(1, args.warmup)):
+        idx.search_batch_uneven(qn, Ks, Ls, out_ids=idn, out_dists=dn)
+    d.barrier()
+    e2e_t = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        idx.search_batch_uneven(qn, Ks, Ls, out_ids=idn, out_dists=dn)
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_s = d.max(sum(e2e_t), device)
+    e2e_qps = nq * d.world * args.steps / e2e_s
+    same_ids = bool(np.array_equal(idn, ids_np))
+
+    # plain per-query GPU path on a sample
+    ns = min(args.plain_sample, nq)
+    for i in range(min(8, ns)):
+        idx.search(wl["queries"][i], int(Ks[i]), int(Ls[i]))
+    plain_same = True
+    t0 = time.perf_counter()
+    for i in range(ns):
+        got, _ = idx.search(wl["queries"][i], int(Ks[i]), int(Ls[i]))
+        plain_same &= bool(np.array_equal(got, ids_np[off[i]:off[i] + Ks[i]]))
+    plain_qps = ns / (time.perf_counter() - t0)
+
+    peak, peak_kind = measured_hbm_peak()
+    traffic, traffic_src = profiled_traffic(args.workload, L_max, nq)
+    mean_step_s = sum(step_ms) / len(step_ms) / 1000.0
+    achieved = bytes_per_step / mean_step_s / 1e9
+    out = {
+        "metric": METRIC, "value": qps, "unit": "queries/s", "n_gpus": d.world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total_s / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": wl["w"].name + " (synthetic, seeded numpy; graph built on the device)",
+        "config": {"workload": wl["spec"]["desc"] + f", {nq} queries per GPU, one "
+                   "graph-captured persistent launch",
+                   "K_counts": {str(k): int((Ks == k).sum()) for k in (1, 10, 100)},
+                   "L_mean": float(Ls.mean()), "L_max": L_max,
+                   "recall@10_K>=10": r10, "recall@1_K=1": r1,
+                   "recall_sample": f"first {len(wl['gt'])} queries ({n10} with K>=10, "
+                                    f"{n1} with K=1)",
+                   "base": list(wl["X"].shape), "graph_R": int(wl["w"].graph_R),
+                   "mean_degree": float((wl["adj"] != 0xFFFFFFFF).sum(1).mean()),
+                   "l2": "inputs larger than L2 (base %.0f MB > 126 MB L2)"
+                         % (wl["X"].numel() * 4 / 1e6),
+                   "parallelism": f"replicas x{d.world}, queries sharded",
+                   "ground_truth": wl["gt_info"],
+                   "tuning": {"warps_per_block": tune["warps_per_block"],
+                              "hash_cap": tune["hash_cap"]}},
+        "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": nq * dim * 4,
+                "d2h_bytes_per_step": total * 8, "ids_equal_device_path": same_ids},
+        "plain_gpu": {"value": plain_qps, "unit": "queries/s", "sample": ns,
+                      "ids_equal_batched": plain_same,
+                      "batched_over_plain": qps / d.world / plain_qps},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                     "traffic_source": traffic_src,
+                     "algorithmic_bytes_per_query": bytes_per_step / nq,
+                     "ndc_per_query": float(ndc.mean()), "hops_per_query": float(hops.mean()),
+                     "distance_evals_per_s": float(ndc.sum()) / mean_step_s,
+                     "device_evals_per_query": float(ndc_dev.mean())},
+        "gpu_launches": args.steps,
+        "launch": "one CUDA graph per step (queue reset, status reset, search kernel)",
+        "clocks": clocks,
+    }
+    if d.rank == 0 and d.world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = time_port_uneven(wl, Ks, Ls, off, ids_np, args.cpu_seconds)
+    plan.close()
+    idx.close()
+    if d.rank == 0:
+        print(json.dumps(out))
+    d.close()
+    return 0
+
+
+def time_port_uneven(wl, Ks, Ls, off, ids_np, seconds):
+    """The oracle's C restatement of SearchArraySimulation, OpenMP over
+    queries with per-query K and L, on a bounded prefix of the batch (the
+    reference's own drivers take one K and L per run)."""
+    from oracle import oracle as O
+    th = cpu_threads()
+    base, adj, ep, metric, q = wl["w"].base, wl["adj"], int(wl["ep"]), wl["metric"], wl["queries"]
+    probe = min(len(q), max(8 * th, 64))
+    t0 = time.perf_counter()
+    O.search(base, adj, ep, metric, q[:probe], Ks=Ks[:probe], Ls=Ls[:probe], nthreads=th)
+    rate = probe / max(1e-6, time.perf_counter() - t0)
+    sample = int(min(len(q), max(probe, rate * seconds)))
+    t0 = time.perf_counter()
+    cids = O.search(base, adj, ep, metric, q[:sample], Ks=Ks[:sample], Ls=Ls[:sample],
+                    nthreads=th)[0]
+    dt = time.perf_counter() - t0
+    n_ids = int(off[sample - 1] + Ks[sample - 1]) if sample else 0
+    return {"value": sample / dt, "unit": "queries/s", "cores": th, "kind": "port",
+            "sample": f"first {sample} of {len(q)} queries, per-query K and L, C restatement "
+                      "of SearchArraySimulation, OpenMP over queries",
+            "ids_equal_gpu": bool(np.array_equal(cids, ids_np[:n_ids]))}
+
 
 def main(argv=None):
     args = parse_args(argv)
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "cfg4":
+        return run_uneven(args)
     return run_ours(args)
 
 

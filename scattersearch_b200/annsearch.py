@@ -49,6 +49,17 @@ def _dptr(x):
     return ctypes.c_void_p(int(x)) if int(x) else None
 
 
+def _out(buf, shape, dtype, name):
+    """A caller's output array, checked, or a new one of ``shape``."""
+    if buf is None:
+        return np.empty(shape, dtype=dtype)
+    n = int(np.prod(shape))
+    if buf.dtype != dtype or not buf.flags.c_contiguous or buf.size < n:
+        raise ValueError(f"{name} must be a C-contiguous {np.dtype(dtype).name} array of "
+                         f"{n} entries")
+    return buf
+
+
 def _query_seed(query_id: int) -> int:
     """Seed of the scatter search's entry points for one reference query id."""
     return (int(query_id) * 0x9E3779B97F4A7C15 + 1) & 0xFFFFFFFFFFFFFFFF
@@ -199,25 +210,23 @@ class ANNSearch:
         e.g. views of pinned buffers) receive the results when given."""
         q = _f32(queries).reshape(-1, self.dimension)
         nq = q.shape[0]
-        ids = out_ids if out_ids is not None else np.empty((nq, K), dtype=np.uint32)
-        dists = out_dists if out_dists is not None else np.empty((nq, K), dtype=np.float32)
-        if ids.dtype != np.uint32 or not ids.flags.c_contiguous or ids.size < nq * K:
-            raise ValueError("out_ids must be a C-contiguous uint32 array of nq*K entries")
-        if dists.dtype != np.float32 or not dists.flags.c_contiguous or dists.size < nq * K:
-            raise ValueError("out_dists must be a C-contiguous float32 array of nq*K entries")
+        ids = _out(out_ids, (nq, K), np.uint32, "out_ids")
+        dists = _out(out_dists, (nq, K), np.float32, "out_dists")
         self._check(self._lib.ss_search_batch(self._h, _ptr(q, _f32p), nq, int(K), int(L),
                                               _ptr(ids, _u32p), _ptr(dists, _f32p)))
         return ids, dists
 
-    def search_batch_uneven(self, queries, Ks, Ls):
-        """Per-query K and L; returns flat ids/dists (query i at sum(Ks[:i]))."""
+    def search_batch_uneven(self, queries, Ks, Ls, out_ids=None, out_dists=None):
+        """Per-query K and L; returns flat ids/dists (query i at sum(Ks[:i])).
+        ``out_ids``/``out_dists`` (C-contiguous uint32/float32 of sum(Ks)
+        entries, e.g. views of pinned buffers) are filled in place."""
         q = _f32(queries).reshape(-1, self.dimension)
         nq = q.shape[0]
         k = np.ascontiguousarray(Ks, dtype=np.int32)
         l = np.ascontiguousarray(Ls, dtype=np.int32)
         total = int(k.sum())
-        ids = np.empty(total, dtype=np.uint32)
-        dists = np.empty(total, dtype=np.float32)
+        ids = _out(out_ids, (total,), np.uint32, "out_ids")
+        dists = _out(out_dists, (total,), np.float32, "out_dists")
         self._check(self._lib.ss_search_batch_uneven(self._h, _ptr(q, _f32p), nq, _ptr(k, _i32p),
                                                      _ptr(l, _i32p), _ptr(ids, _u32p),
                                                      _ptr(dists, _f32p)))

@@ -85,23 +85,37 @@ def apply(index, L: int, path: str = DEFAULT_CACHE, device=None) -> dict | None:
 
 
 def autotune(index, queries, K: int, L: int, reps: int = 3, path: str | None = DEFAULT_CACHE,
-             device=None, wpb_candidates=WPB_CANDIDATES, hash_caps=None) -> dict:
+             device=None, wpb_candidates=WPB_CANDIDATES, hash_caps=None, Ks=None, Ls=None,
+             out_off=None) -> dict:
     """Times every (warps_per_block, hash_cap) candidate on ``queries`` (a
     CUDA tensor, nq x dim) and sets the fastest on ``index``.  Raises if two
     candidates return different ids.  Returns the choice with the timing
-    table; stores it in the cache at ``path`` (None: no cache)."""
+    table; stores it in the cache at ``path`` (None: no cache).
+
+    For a batch with per-query K and L, pass the device arrays ``Ks``, ``Ls``
+    and ``out_off`` (as for ``search_batch_device``); ``K`` is then the total
+    number of result slots and ``L`` the largest L of the batch."""
     import torch
     nq = int(queries.shape[0])
     dev = queries.device
-    ids = torch.empty((nq, K), dtype=torch.int32, device=dev)
+    uneven = Ks is not None
+    ids = torch.empty((K,) if uneven else (nq, K), dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream(dev)
+
+    def launch():
+        if uneven:
+            index.search_batch_device(queries, nq, ids, None, Ks=Ks, Ls=Ls, out_off=out_off,
+                                      L_max=L, stream=stream.cuda_stream)
+        else:
+            index.search_batch_device(queries, nq, ids, None, K=K, L=L,
+                                      stream=stream.cuda_stream)
+
     ref = None
     table = []
     for hc in (hash_caps or hash_candidates(L)):
         for wpb in wpb_candidates:
             index.set_tuning(wpb, hc, 0)
-            index.search_batch_device(queries, nq, ids, None, K=K, L=L,
-                                      stream=stream.cuda_stream)
+            launch()
             stream.synchronize()
             got = ids.cpu().numpy()
             if ref is None:
@@ -113,8 +127,7 @@ def autotune(index, queries, K: int, L: int, reps: int = 3, path: str | None = D
                 a = torch.cuda.Event(enable_timing=True)
                 b = torch.cuda.Event(enable_timing=True)
                 a.record(stream)
-                index.search_batch_device(queries, nq, ids, None, K=K, L=L,
-                                          stream=stream.cuda_stream)
+                launch()
                 b.record(stream)
                 stream.synchronize()
                 times.append(a.elapsed_time(b))
@@ -122,7 +135,8 @@ def autotune(index, queries, K: int, L: int, reps: int = 3, path: str | None = D
     best = min(table, key=lambda r: r["ms"])
     index.set_tuning(best["warps_per_block"], best["hash_cap"], 0)
     choice = {"warps_per_block": best["warps_per_block"], "hash_cap": best["hash_cap"],
-              "ms": best["ms"], "sample_queries": nq, "K": K, "L": L}
+              "ms": best["ms"], "sample_queries": nq, "K": "per query" if uneven else K,
+              "L": L}
     if path:
         save_choice(tuning_key(_gpu_name(device if device is not None else dev),
                                index.dimension, index.rstride, L), choice, path)

@@ -288,8 +288,10 @@ def repair_connectivity(adj: np.ndarray, knn_ids: np.ndarray, ep: int, X: torch.
 
 @torch.no_grad()
 def build_graph(X, R: int = 32, knn_k: int = 64, device: str | torch.device | None = None,
-                reverse: bool = True, repair: bool = True):
+                reverse: bool = True, repair: bool = True, knn_budget_bytes: float = 6e9):
     """Builds an out-degree <= R graph over X (n x d float32, numpy or torch).
+    ``knn_budget_bytes`` bounds the distance block of one k-NN chunk (larger
+    blocks mean fewer, more efficient launches on large bases).
     Returns (adj uint32 n x R padded with 0xFFFFFFFF, entry point)."""
     dev = torch.device(device) if device is not None else (
         torch.device("cuda") if torch.cuda.is_available() else torch.device("cpu"))
@@ -297,7 +299,7 @@ def build_graph(X, R: int = 32, knn_k: int = 64, device: str | torch.device | No
     Xt = Xt.to(dev, dtype=torch.float32).contiguous()
     n = Xt.shape[0]
     k = min(knn_k, n - 1)
-    ids, d = knn(Xt, k)
+    ids, d = knn(Xt, k, budget_bytes=knn_budget_bytes)
     adj = mrng_prune(Xt, ids, d, R)
     if reverse:
         adj = add_reverse_edges(Xt, adj, R)

@@ -355,6 +355,11 @@ def test_graph_captured_uneven_plan(oracle_lib):
     dK, dL, doff = (torch.as_tensor(x).cuda() for x in (Ks, Ls, off))
     ids = torch.empty(total, dtype=torch.int32, device="cuda")
     d = torch.empty(total, dtype=torch.float32, device="cuda")
+    # the autotuner over the uneven batch keeps the ids
+    from scattersearch_b200 import autotune
+    choice = autotune.autotune(idx, q, total, 512, reps=1, path=None, Ks=dK, Ls=dL,
+                               out_off=doff, wpb_candidates=(2, 8), hash_caps=(1024, 4096))
+    assert len(choice["table"]) == 4
     plan = idx.plan_batch_uneven_device(q, nq, dK, dL, doff, 512, ids, d)
     o_ids, o_d, _, _ = oracle_lib.search(fx["base"], fx["adj"], int(fx["ep"]), 0, Q, Ks=Ks, Ls=Ls)
     s = torch.cuda.current_stream()
