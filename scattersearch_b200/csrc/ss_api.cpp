@@ -71,7 +71,8 @@ struct DevBuf {
 // Per-caller launch state: one stream plus the buffers a search needs.
 struct SearchCtx {
   cudaStream_t stream = nullptr;
-  DevBuf q, ids, dists, Ks, Ls, off, counter, status, ndc, hops, spill, bf_q, bf_cand;
+  DevBuf q, ids, dists, Ks, Ls, off, counter, status, ndc, hops, spill, bf_q, bf_qpack, bf_cand,
+      bf_err;
   std::vector<int32_t> h_status;
   ~SearchCtx() {
     if (stream) cudaStreamDestroy(stream);
@@ -101,10 +102,11 @@ struct ss_index {
   SearchCtx dev_ctx;
   uint32_t dev_last_nq = 0;
 
-  // squared row norms for the L2 brute force, computed on first use
+  // squared row norms (L2) and the base rows in packed tensor-core tiles for
+  // the brute force, built on first use
   std::mutex norm_mu;
-  DevBuf xnorm;
-  bool have_norms = false;
+  DevBuf xnorm, bpack;
+  bool have_norms = false, have_bpack = false;
 
   // launch tuning (set by the autotuner through ss_set_tuning); 0 = automatic
   int warps_per_block = 0;
@@ -871,27 +873,52 @@ int bruteforce_common(ss_index *h, SearchCtx *c, const float *d_queries, size_t 
     xnorm = h->xnorm.as<float>();
   }
   ssb::BrutePlan bp = ssb::plan_bruteforce(h->n, nq, k, h->sm_count);
+  const float *bpack = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(h->norm_mu);
+    if (!h->have_bpack) {
+      SS_CUDA(h, h->bpack.ensure(ssb::bruteforce_pack_bytes(h->n, h->dim, true)), "packed base");
+      SS_CUDA(h, ssb::launch_pack(h->base.as<float>(), h->n, pitch, h->dim, true,
+                                  h->bpack.as<float>(), stream),
+              "base packing");
+      h->have_bpack = true;
+    }
+    bpack = h->bpack.as<float>();
+  }
+  const uint32_t lists = 2 * bp.splits;
   SS_CUDA(h, c->bf_q.ensure((size_t)nq * pitch * 4), "query buffer");
-  SS_CUDA(h, c->bf_cand.ensure((size_t)nq * bp.splits * bp.C * 8), "candidate buffer");
+  SS_CUDA(h, c->bf_qpack.ensure(ssb::bruteforce_pack_bytes(nq, h->dim, false)), "packed queries");
+  SS_CUDA(h, c->bf_cand.ensure((size_t)nq * lists * bp.list_cap * 8), "candidate buffer");
+  SS_CUDA(h, c->bf_err.ensure(4), "error word");
+  SS_CUDA(h, cudaMemsetAsync(c->bf_err.p, 0, 4, stream), "error word clear");
   SS_CUDA(h, cudaMemsetAsync(c->bf_q.p, 0, (size_t)nq * pitch * 4, stream), "query clear");
   SS_CUDA(h, cudaMemcpy2DAsync(c->bf_q.p, (size_t)pitch * 4, d_queries, qstride * 4,
                                (size_t)h->dim * 4, nq, cudaMemcpyDeviceToDevice, stream),
           "query copy");
+  SS_CUDA(h, ssb::launch_pack(d_queries, nq, (uint32_t)qstride, h->dim, false,
+                              c->bf_qpack.as<float>(), stream),
+          "query packing");
   ssb::BruteArgs a{};
   a.base = h->base.as<float>();
   a.n = h->n;
   a.nb = h->nb;
   a.queries = c->bf_q.as<float>();
   a.nq = nq;
+  a.qpack = c->bf_qpack.as<float>();
+  a.bpack = bpack;
+  a.kblocks = ssb::bruteforce_kblocks(h->dim);
   a.xnorm = xnorm;
   a.metric = h->metric;
   a.k = k;
   a.C = bp.C;
   a.splits = bp.splits;
   a.rows_per_split = bp.rows_per_split;
+  a.lists = lists;
+  a.list_stride = bp.list_cap;
   a.cand = c->bf_cand.as<uint64_t>();
   a.ids = d_ids;
   a.dists = d_dists;
+  a.err = c->bf_err.as<uint32_t>();
   SS_CUDA(h, ssb::launch_bruteforce(a, h->view(), stream), "brute-force launch");
   return SS_OK;
 }
@@ -928,12 +955,17 @@ int ss_bruteforce(ss_index *h, const float *queries, uint32_t nq, int k, uint32_
   rc = bruteforce_common(h, c, c->q.as<float>(), h->dim, nq, k, c->ids.as<uint32_t>(),
                          c->dists.as<float>(), c->stream);
   if (rc) return rc;
+  uint32_t err = 0;
   SS_CUDA(h, cudaMemcpyAsync(ids, c->ids.p, total * 4, cudaMemcpyDeviceToHost, c->stream),
           "ids download");
   if (dists)
     SS_CUDA(h, cudaMemcpyAsync(dists, c->dists.p, total * 4, cudaMemcpyDeviceToHost, c->stream),
             "dists download");
+  SS_CUDA(h, cudaMemcpyAsync(&err, c->bf_err.p, 4, cudaMemcpyDeviceToHost, c->stream),
+          "error word download");
   SS_CUDA(h, cudaStreamSynchronize(c->stream), "brute force");
+  if (err)
+    return set_err(h, SS_ERR_TIMEOUT, "a brute-force pipeline wait ran out; results are invalid");
   return SS_OK;
 }
 

@@ -110,25 +110,38 @@ cudaError_t launch_count_failed(const int32_t *status, uint32_t nq, uint32_t *fa
 
 // ---- brute-force k-NN (ss_bruteforce.cu) --------------------------------
 struct BruteArgs {
-  const float *base;      // n x (nb*8), padded rows
+  const float *base;      // n x (nb*8), padded rows (exact re-rank)
   uint32_t n, nb;
-  const float *queries;   // nq x (nb*8), padded with zeros
+  const float *queries;   // nq x (nb*8), padded with zeros (exact re-rank)
   uint32_t nq;
+  const float *qpack;     // queries in packed tensor-core tiles (launch_pack)
+  const float *bpack;     // base rows in packed tensor-core tiles
+  uint32_t kblocks;       // 32-float k-blocks per row
   const float *xnorm;     // n squared norms (L2 only)
   int metric;
-  int k, C;               // results per query; candidates kept per split (32/64/128)
+  int k, C;               // results per query; candidates kept per list (32/64/128)
   uint32_t splits, rows_per_split;
-  uint64_t *cand;         // nq x splits x C scratch
+  uint32_t lists, list_stride;  // candidate lists per query (2 per split); entries per list
+  uint64_t *cand;         // nq x lists x list_stride scratch
   uint32_t *ids;          // nq x k
   float *dists;           // nq x k, may be null
+  uint32_t *err;          // set to 1 when a bounded wait ran out; may be null
 };
 struct BrutePlan {
   int C;
+  uint32_t list_cap;      // entries per candidate list
   uint32_t splits, rows_per_split;
+  uint32_t kblocks;
 };
 // Largest k the brute force accepts (candidates kept = k + 16 <= 128).
 constexpr int kBruteMaxK = 112;
 BrutePlan plan_bruteforce(uint32_t n, uint32_t nq, int k, int sm_count);
+uint32_t bruteforce_kblocks(uint32_t dim);
+// Bytes of `rows` rows of width `dim` in packed tensor-core tiles (base side:
+// 256-row tiles; query side: 128-row tiles).
+size_t bruteforce_pack_bytes(uint32_t rows, uint32_t dim, bool base_side);
+cudaError_t launch_pack(const float *src, uint32_t rows, uint32_t pitch, uint32_t dim,
+                        bool base_side, float *dst, cudaStream_t s);
 cudaError_t launch_norms(const float *base, uint32_t n, uint32_t pitch, float *out,
                          cudaStream_t s);
 cudaError_t launch_bruteforce(const BruteArgs &a, const GraphView &g, cudaStream_t s);
