@@ -223,10 +223,10 @@ def build_workload(args, rank, world, device):
     log(f"data {w.base.shape} queries {queries.shape} in {time.time() - t0:.1f}s")
     t0 = time.time()
     X = torch.from_numpy(w.base).to(device)
-    # large bases: bigger k-NN distance blocks (fewer launches), within HBM
-    budget = 24e9 if X.shape[0] > 2_000_000 and device != "cpu" else 6e9
+    # config 4 takes its exact 64-NN from the library's tensor-core brute force
+    backend = "bruteforce" if spec["cfg"] == 4 and device != "cpu" else "torch"
     adj, ep = graph.build_graph(X, R=w.graph_R, knn_k=w.graph_knn, device=device,
-                                knn_budget_bytes=budget)
+                                knn_backend=backend)
     log(f"graph R={w.graph_R} ep={ep} mean degree {(adj != 0xFFFFFFFF).sum(1).mean():.1f} "
         f"in {time.time() - t0:.1f}s")
     Q = torch.from_numpy(queries).to(device)

@@ -50,6 +50,42 @@ def knn(X: torch.Tensor, k: int, chunk: int | None = None, budget_bytes: float =
 
 
 @torch.no_grad()
+def knn_tensor_cores(X: torch.Tensor, k: int, chunk: int = 1 << 18):
+    """Exact k nearest neighbours of every row of X among the rows of X
+    (squared L2, ties by smaller id), excluding the row itself, from the
+    library's tensor-core brute force (ss_bruteforce_device) on X's CUDA
+    device.  Returns (ids int64 [n,k], sq. dists [n,k]) like ``knn``."""
+    from .annsearch import ANNSearch
+    n, dim = X.shape
+    if k + 1 > 112:
+        raise ValueError("the brute force returns at most 112 neighbours")
+    X = X.contiguous()
+    dev = X.device.index if X.device.index is not None else -1
+    idx = ANNSearch(dim, n, X, 0, device=dev, base_on_device=True)
+    out_i = torch.empty((n, k), dtype=torch.int64, device=X.device)
+    out_d = torch.empty((n, k), dtype=torch.float32, device=X.device)
+    ids = torch.empty((min(chunk, n), k + 1), dtype=torch.int32, device=X.device)
+    dists = torch.empty((min(chunk, n), k + 1), dtype=torch.float32, device=X.device)
+    stream = torch.cuda.current_stream(X.device).cuda_stream
+    try:
+        for s in range(0, n, chunk):
+            e = min(n, s + chunk)
+            idx.bruteforce_device(X[s:e], e - s, k + 1, ids, dists, stream=stream)
+            got = ids[:e - s].to(torch.int64) & 0xFFFFFFFF
+            rows = torch.arange(s, e, device=X.device)
+            # drop the row itself; when k+1 exact duplicates of it with smaller
+            # ids push it out of the list, drop the last entry instead
+            drop = got == rows[:, None]
+            drop[~drop.any(1), -1] = True
+            out_i[s:e] = got[~drop].view(e - s, k)
+            out_d[s:e] = dists[:e - s][~drop].view(e - s, k)
+        torch.cuda.synchronize(X.device)
+    finally:
+        idx.close()
+    return out_i, out_d
+
+
+@torch.no_grad()
 def bruteforce(X: torch.Tensor, Q: torch.Tensor, k: int, metric: int, chunk: int | None = None,
                budget_bytes: float = 6e9, exact_dtype=torch.float64):
     """Exact top-k of Q against X: float32 candidate scan, then the top
@@ -288,10 +324,12 @@ def repair_connectivity(adj: np.ndarray, knn_ids: np.ndarray, ep: int, X: torch.
 
 @torch.no_grad()
 def build_graph(X, R: int = 32, knn_k: int = 64, device: str | torch.device | None = None,
-                reverse: bool = True, repair: bool = True, knn_budget_bytes: float = 6e9):
+                reverse: bool = True, repair: bool = True, knn_budget_bytes: float = 6e9,
+                knn_backend: str = "torch"):
     """Builds an out-degree <= R graph over X (n x d float32, numpy or torch).
-    ``knn_budget_bytes`` bounds the distance block of one k-NN chunk (larger
-    blocks mean fewer, more efficient launches on large bases).
+    ``knn_backend``: "torch" (FP32 matmul + top-k, any device; its
+    ``knn_budget_bytes`` bounds one distance block) or "bruteforce" (the
+    library's exact tensor-core k-NN, CUDA only).
     Returns (adj uint32 n x R padded with 0xFFFFFFFF, entry point)."""
     dev = torch.device(device) if device is not None else (
         torch.device("cuda") if torch.cuda.is_available() else torch.device("cpu"))
@@ -299,7 +337,12 @@ def build_graph(X, R: int = 32, knn_k: int = 64, device: str | torch.device | No
     Xt = Xt.to(dev, dtype=torch.float32).contiguous()
     n = Xt.shape[0]
     k = min(knn_k, n - 1)
-    ids, d = knn(Xt, k, budget_bytes=knn_budget_bytes)
+    if knn_backend == "bruteforce":
+        ids, d = knn_tensor_cores(Xt, k)
+    elif knn_backend == "torch":
+        ids, d = knn(Xt, k, budget_bytes=knn_budget_bytes)
+    else:
+        raise ValueError(f"unknown k-NN backend {knn_backend!r}")
     adj = mrng_prune(Xt, ids, d, R)
     if reverse:
         adj = add_reverse_edges(Xt, adj, R)
