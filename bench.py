@@ -263,8 +263,8 @@ def ground_truth(X, Q, metric, device, k=10):
     ms = a.elapsed_time(b)
     idx.close()
     return ids.cpu().numpy().view(np.uint32), {
-        "kernel": "bf_candidates_kernel (TF32 mma.sync, three-term products, FP32 accumulate) "
-                  "+ bf_rerank_kernel (exact FP32 distance, ties by id)",
+        "kernel": "bf_tc_candidates_kernel (tcgen05.mma kind::tf32 into TMEM, three-term "
+                  "products, FP32 accumulate) + bf_rerank_kernel (exact FP32 distance, ties by id)",
         "ms": ms, "tensor_tflops": 3 * 2 * nq * n * dim / ms / 1e9,
         "queries": int(nq), "base": int(n)}
 

@@ -74,3 +74,27 @@ def test_bruteforce_small_index_and_limits():
     with pytest.raises(SearchError):
         idx.bruteforce(X[:1], 113)
     idx.close()
+
+
+def test_graph_knn_from_the_brute_force(oracle_lib):
+    """graph.knn_tensor_cores: each row's k nearest other rows, exactly as the
+    oracle's scan ranks them (ties by id), with the row itself dropped."""
+    import torch
+    from scattersearch_b200 import graph
+    rng = np.random.default_rng(8)
+    X = rng.standard_normal((6000, 40)).astype(np.float32)
+    X[100] = X[7]  # an exact duplicate: row 100's nearest is row 7 at distance 0
+    k = 24
+    ids, d = graph.knn_tensor_cores(torch.from_numpy(X).cuda(), k, chunk=2048)
+    ids, d = ids.cpu().numpy(), d.cpu().numpy()
+    sample = np.r_[0:64, 100, 5000:5064]
+    o_ids, o_d = oracle_lib.bruteforce(X, X[sample], k + 1, 0)
+    for row, oi, od in zip(sample, o_ids.astype(np.int64), o_d):
+        keep = oi != row
+        if keep.all():
+            keep[-1] = False
+        assert np.array_equal(ids[row], oi[keep]), row
+        assert _same_bits(d[row], od[keep]), row
+    assert ids[100][0] == 7 and d[100][0] == 0.0
+    adj, ep = graph.build_graph(X, R=16, knn_k=k, device="cuda", knn_backend="bruteforce")
+    assert adj.shape == (6000, 16) and 0 <= ep < 6000
