@@ -256,6 +256,13 @@ int ss_search_scatter_batch_device(ss_index *h, const float *queries, uint32_t n
  * blocks_per_sm_cap: limit on resident CTAs per SM (0 = occupancy limit). */
 int ss_set_tuning(ss_index *h, int warps_per_block, int hash_cap, int blocks_per_sm_cap);
 
+/* Row stages shared by the query teams of one CTA of the batched kernel
+ * (0 = each team has its own 16-row stage; n > 0 = a pool of n stages per
+ * CTA, used when the CTA has more than n teams).  A team holds a stage only
+ * while its rows are copied in and its distances computed, so a shared pool
+ * leaves room for more teams per SM.  Results never depend on it. */
+int ss_set_shared_stages(ss_index *h, int stages_per_block);
+
 /* ---- exact brute force -------------------------------------------------- */
 
 /* Exact k nearest base rows of each query by brute force (no graph needed);

@@ -1,11 +1,12 @@
 """Launch autotuner of the batched search kernel.
 
 The reference has no tunables beyond compile-time macros.  Here the batched
-warp-per-query kernel exposes two layout choices that change speed but never
-results: how many query teams share a CTA (``warps_per_block``) and the size
-of each query's shared-memory visited table (``hash_cap``; a smaller table
-fits more teams per SM but forgets more visited ids, which are then evaluated
-again).  ``autotune`` times candidate pairs on a sample of the caller's
+warp-per-query kernel exposes three layout choices that change speed but never
+results: how many query teams share a CTA (``warps_per_block``), how many row
+stages those teams share (``shared_stages``; 0 = one per team, fewer stages
+than teams leave room for more teams per SM) and the size of each query's
+shared-memory visited table (``hash_cap``; a smaller table fits more teams
+per SM but forgets more visited ids, which are then evaluated again).  ``autotune`` times candidate pairs on a sample of the caller's
 queries with CUDA events, checks that every candidate returns the same ids,
 and keeps the fastest.  Choices are cached per (GPU name, dim, adjacency row
 stride, L rounded up to a power of two) in a JSON file, so ``apply`` can
@@ -22,6 +23,8 @@ import numpy as np
 DEFAULT_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "scattersearch_b200",
                              "tuning.json")
 WPB_CANDIDATES = (1, 2, 4, 8)
+# (teams per CTA, shared row stages) layouts tried besides one stage per team
+SHARED_CANDIDATES = ((2, 1), (4, 2), (4, 3), (8, 3), (8, 4), (8, 5))
 _lock = threading.Lock()
 
 
@@ -80,14 +83,17 @@ def apply(index, L: int, path: str = DEFAULT_CACHE, device=None) -> dict | None:
     key = tuning_key(_gpu_name(device), index.dimension, index.rstride, L)
     choice = load_cache(path).get(key)
     if choice:
-        index.set_tuning(int(choice["warps_per_block"]), int(choice["hash_cap"]), 0)
+        index.set_tuning(int(choice["warps_per_block"]), int(choice["hash_cap"]), 0,
+                         int(choice.get("shared_stages", 0)))
     return choice
 
 
 def autotune(index, queries, K: int, L: int, reps: int = 3, path: str | None = DEFAULT_CACHE,
              device=None, wpb_candidates=WPB_CANDIDATES, hash_caps=None, Ks=None, Ls=None,
-             out_off=None) -> dict:
-    """Times every (warps_per_block, hash_cap) candidate on ``queries`` (a
+             out_off=None, shared_candidates=SHARED_CANDIDATES) -> dict:
+    """Times every (warps_per_block, shared_stages, hash_cap) candidate --
+    each of ``wpb_candidates`` with a stage per team, and each pair of
+    ``shared_candidates`` -- on ``queries`` (a
     CUDA tensor, nq x dim) and sets the fastest on ``index``.  Raises if two
     candidates return different ids.  Returns the choice with the timing
     table; stores it in the cache at ``path`` (None: no cache).
@@ -112,16 +118,18 @@ def autotune(index, queries, K: int, L: int, reps: int = 3, path: str | None = D
 
     ref = None
     table = []
+    layouts = [(w, 0) for w in wpb_candidates] + list(shared_candidates or ())
     for hc in (hash_caps or hash_candidates(L)):
-        for wpb in wpb_candidates:
-            index.set_tuning(wpb, hc, 0)
+        for wpb, stages in layouts:
+            index.set_tuning(wpb, hc, 0, stages)
             launch()
             stream.synchronize()
             got = ids.cpu().numpy()
             if ref is None:
                 ref = got.copy()
             elif not np.array_equal(got, ref):
-                raise RuntimeError(f"ids differ under warps_per_block={wpb}, hash_cap={hc}")
+                raise RuntimeError(f"ids differ under warps_per_block={wpb}, "
+                                   f"shared_stages={stages}, hash_cap={hc}")
             times = []
             for _ in range(reps):
                 a = torch.cuda.Event(enable_timing=True)
@@ -131,12 +139,13 @@ def autotune(index, queries, K: int, L: int, reps: int = 3, path: str | None = D
                 b.record(stream)
                 stream.synchronize()
                 times.append(a.elapsed_time(b))
-            table.append({"warps_per_block": wpb, "hash_cap": hc, "ms": float(np.median(times))})
+            table.append({"warps_per_block": wpb, "shared_stages": stages, "hash_cap": hc,
+                          "ms": float(np.median(times))})
     best = min(table, key=lambda r: r["ms"])
-    index.set_tuning(best["warps_per_block"], best["hash_cap"], 0)
-    choice = {"warps_per_block": best["warps_per_block"], "hash_cap": best["hash_cap"],
-              "ms": best["ms"], "sample_queries": nq, "K": "per query" if uneven else K,
-              "L": L}
+    index.set_tuning(best["warps_per_block"], best["hash_cap"], 0, best["shared_stages"])
+    choice = {"warps_per_block": best["warps_per_block"], "shared_stages": best["shared_stages"],
+              "hash_cap": best["hash_cap"], "ms": best["ms"], "sample_queries": nq,
+              "K": "per query" if uneven else K, "L": L}
     if path:
         save_choice(tuning_key(_gpu_name(device if device is not None else dev),
                                index.dimension, index.rstride, L), choice, path)

@@ -112,6 +112,7 @@ struct ss_index {
   int warps_per_block = 0;
   int hash_cap_override = 0;
   int blocks_per_sm_cap = 0;
+  int shared_stages = 0;  // row stages shared by a CTA's teams (0 = one per team)
 
   ssb::GraphView view() const {
     ssb::GraphView g;
@@ -237,13 +238,25 @@ int persistent_blocks(ss_index *h, const ssb::SmemPlan &p, int wpb, uint32_t nq)
   return (int)std::max(1L, std::min(full, need));
 }
 
+// Row stages shared by a CTA of `wpb` teams under the tuning of `h` (0 =
+// a private stage per team; sharing needs fewer stages than teams).
+int stages_for(const ss_index *h, int wpb) {
+  return h->shared_stages > 0 && h->shared_stages < wpb ? h->shared_stages : 0;
+}
+
 // Query teams per CTA: the tuned value when set, else the candidate (1, 2,
-// 4, 8) that keeps the most teams resident per SM (ties: larger CTAs).
-int choose_wpb(ss_index *h, const ssb::SmemPlan &p) {
-  auto fits = [&](int w) { return (size_t)p.words_per_team * 4 * w <= 227 * 1024; };
+// 4, 8) that keeps the most teams resident per SM (ties: larger CTAs).  The
+// plan's stage layout is set to match.
+int choose_wpb(ss_index *h, ssb::SmemPlan &p) {
+  auto fits = [&](int w) {
+    ssb::SmemPlan q = p;
+    ssb::share_stages(q, stages_for(h, w));
+    return ssb::warp_search_smem_bytes(q, w) <= 227 * 1024;
+  };
   if (h->warps_per_block > 0) {
     int wpb = h->warps_per_block;
     while (wpb > 1 && !fits(wpb)) wpb >>= 1;
+    ssb::share_stages(p, stages_for(h, wpb));
     return wpb;
   }
   int best = 1, best_teams = -1;
@@ -255,6 +268,7 @@ int choose_wpb(ss_index *h, const ssb::SmemPlan &p) {
       best = w;
     }
   }
+  ssb::share_stages(p, stages_for(h, best));
   return best;
 }
 
@@ -266,7 +280,7 @@ int launch_batch(ss_index *h, SearchCtx *c, const float *d_q, uint32_t nq, const
   ssb::GraphView g = h->view();
   ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, h->hash_cap_override);
   const int wpb = choose_wpb(h, plan);
-  if ((size_t)plan.words_per_team * 4 * wpb > 227 * 1024)
+  if (ssb::warp_search_smem_bytes(plan, wpb) > 227 * 1024)
     return set_err(h, SS_ERR_UNSUPPORTED, "L=%d needs %u bytes of shared memory per query",
                    L_max, plan.words_per_team * 4);
   int blocks = persistent ? persistent_blocks(h, plan, wpb, nq)
@@ -439,7 +453,7 @@ int server_launch(ss_index *h, const float *d_q, uint32_t nq, const int32_t *d_K
   ssb::GraphView g = h->view();
   ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, h->hash_cap_override);
   const int wpb = choose_wpb(h, plan);
-  if ((size_t)plan.words_per_team * 4 * wpb > 227 * 1024)
+  if (ssb::warp_search_smem_bytes(plan, wpb) > 227 * 1024)
     return set_err(h, SS_ERR_UNSUPPORTED, "L=%d needs %u bytes of shared memory per query",
                    L_max, plan.words_per_team * 4);
   const int blocks = persistent_blocks(h, plan, wpb, nq);
@@ -789,7 +803,7 @@ int ss_plan_create_uneven(ss_index *h, const float *queries, uint32_t nq, const 
   ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, h->hash_cap_override);
   const int wpb = choose_wpb(h, plan);
   const int blocks = persistent_blocks(h, plan, wpb, nq);
-  if ((size_t)plan.words_per_team * 4 * wpb > 227 * 1024 || blocks <= 0) {
+  if (ssb::warp_search_smem_bytes(plan, wpb) > 227 * 1024 || blocks <= 0) {
     plan_free(p);
     cudaStreamDestroy(cs);
     return set_err(h, SS_ERR_UNSUPPORTED, "L=%d cannot be planned on this device", L_max);
@@ -1062,7 +1076,7 @@ int ss_search_batch_noalloc(ss_index *h, const float *queries, uint32_t nq, int 
   ssb::GraphView g = h->view();
   ssb::SmemPlan plan = ssb::plan_warp_smem(g, L, h->hash_cap_override);
   const int wpb = choose_wpb(h, plan);
-  if ((size_t)plan.words_per_team * 4 * wpb > 227 * 1024)
+  if (ssb::warp_search_smem_bytes(plan, wpb) > 227 * 1024)
     return set_err(h, SS_ERR_UNSUPPORTED, "L=%d needs %u bytes of shared memory per query", L,
                    plan.words_per_team * 4);
   const int blocks = persistent_blocks(h, plan, wpb, nq);
@@ -1165,6 +1179,14 @@ int ss_set_tuning(ss_index *h, int warps_per_block, int hash_cap, int blocks_per
   h->warps_per_block = warps_per_block;
   h->hash_cap_override = hash_cap > 0 ? hash_cap : 0;
   h->blocks_per_sm_cap = blocks_per_sm_cap > 0 ? blocks_per_sm_cap : 0;
+  return SS_OK;
+}
+
+int ss_set_shared_stages(ss_index *h, int stages_per_block) {
+  if (!h) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null index handle");
+  if (stages_per_block < 0 || stages_per_block > 32)
+    return set_err(h, SS_ERR_INVALID_ARGUMENT, "stages_per_block must be in [0, 32]");
+  h->shared_stages = stages_per_block;
   return SS_OK;
 }
 

@@ -54,6 +54,7 @@ struct SmemPlan {
   uint32_t stage_split; // warp kernel: 1 = whole rows, 2 = rows staged in two halves
   uint32_t stage_row_words;  // warp kernel: floats per staged row
   uint32_t stage_words; // warp kernel: size of the row stage
+  uint32_t shared_stages;  // warp kernel: row stages shared by a CTA's teams (0 = one per team)
   uint32_t words_per_team;
 };
 
@@ -68,6 +69,11 @@ enum : int32_t {
 
 // Plans shared memory for a warp-per-query launch.
 SmemPlan plan_warp_smem(const GraphView &g, int L_max, int hash_cap_override);
+// Lets the teams of a CTA share `stages` row stages (0: a private stage per
+// team); updates words_per_team.
+void share_stages(SmemPlan &p, int stages);
+// Dynamic shared memory of a warp-kernel CTA of `warps_per_block` teams.
+size_t warp_search_smem_bytes(const SmemPlan &p, int warps_per_block);
 // Plans shared memory for a CTA-per-query launch with `width` expansion warps.
 SmemPlan plan_intra_smem(const GraphView &g, int L_max, int width, int hash_cap_override);
 

@@ -273,10 +273,15 @@ struct WarpSmem {
 
 __device__ __forceinline__ WarpSmem carve_warp(uint32_t *base, const SmemPlan &p) {
   WarpSmem s;
-  s.stage = reinterpret_cast<float *>(base);
-  base += p.stage_words;
-  s.bar = reinterpret_cast<uint64_t *>(base);
-  base += 4;
+  if (p.shared_stages == 0) {
+    s.stage = reinterpret_cast<float *>(base);
+    base += p.stage_words;
+    s.bar = reinterpret_cast<uint64_t *>(base);
+    base += 4;
+  } else {  // the CTA's stage pool holds the stages and their mbarriers
+    s.stage = nullptr;
+    s.bar = nullptr;
+  }
   s.q = reinterpret_cast<float *>(base);
   base += p.q_words;
   s.pk = base;
@@ -321,7 +326,91 @@ struct RowStage {
   uint32_t bar;     // shared address of the mbarrier
   uint32_t phase;   // parity of the phase being filled
   bool broken;      // a wait timed out: the stage may still be written to
+  float *buf;       // the stage's rows
+  int slot;         // pool slot held (shared stages), -1 when none
 };
+
+// Stage pool of a CTA whose teams share row stages (SmemPlan::shared_stages
+// > 0): `count` stages, each with its mbarrier and the parity of its next
+// phase, and a bit mask of free stages.  A team takes a stage just before it
+// starts copying rows and gives it back once the distances of its last pass
+// are computed, so a stage is held only over copy latency and distance
+// arithmetic and the CTA needs fewer stages than teams.
+struct StagePool {
+  float *stages;      // count x stage_words floats
+  uint32_t bar0;      // shared address of the first mbarrier (8 bytes apart)
+  uint32_t *phases;   // count words
+  uint32_t *mask;     // bit i set = stage i free
+  uint32_t count, stage_words;
+};
+
+// Words of the CTA-wide stage pool region (0 with private stages).
+__host__ __device__ __forceinline__ uint32_t stage_pool_words(const SmemPlan &p) {
+  if (p.shared_stages == 0) return 0;
+  const uint32_t w = p.shared_stages * p.stage_words + 2 * p.shared_stages + p.shared_stages + 1;
+  return (w + 31u) & ~31u;
+}
+
+__device__ __forceinline__ StagePool carve_pool(uint32_t *base, const SmemPlan &p) {
+  StagePool sp;
+  sp.count = p.shared_stages;
+  sp.stage_words = p.stage_words;
+  sp.stages = reinterpret_cast<float *>(base);
+  uint32_t *b = base + p.shared_stages * p.stage_words;  // 8-byte aligned (stage_words % 32 == 0)
+  sp.bar0 = (uint32_t)__cvta_generic_to_shared(b);
+  sp.phases = b + 2 * p.shared_stages;
+  sp.mask = sp.phases + p.shared_stages;
+  return sp;
+}
+
+// Takes a free stage of the pool for this team (no-op with a private stage
+// or when one is held).  Lane 0 claims a free bit with compare-and-swap,
+// spinning (bounded) while every stage is in use.  False when the limit ran
+// out; the team then holds nothing.
+__device__ __forceinline__ bool stage_acquire(RowStage &st, const StagePool &sp, int lane) {
+  if (sp.count == 0 || st.slot >= 0) return true;
+  int got = -1;
+  uint32_t phase = 0;
+  if (lane == 0) {
+    volatile uint32_t *vm = sp.mask;
+    for (uint32_t spin = 0; spin < kStageWaitLimit && got < 0; ++spin) {
+      const uint32_t m = *vm;
+      if (m == 0u) {
+        __nanosleep(32);
+        continue;
+      }
+      const int i = __ffs(m) - 1;
+      if (atomicCAS(sp.mask, m, m & ~(1u << i)) == m) got = i;
+    }
+    if (got >= 0) {
+      __threadfence_block();
+      phase = *(volatile uint32_t *)(sp.phases + got);
+    }
+  }
+  got = __shfl_sync(kFull, got, 0);
+  phase = __shfl_sync(kFull, phase, 0);
+  if (got < 0) return false;
+  st.slot = got;
+  st.buf = sp.stages + (size_t)got * sp.stage_words;
+  st.bar = sp.bar0 + 8u * (uint32_t)got;
+  st.phase = phase;
+  return true;
+}
+
+// Gives a pool stage back once its copies have landed and its rows are
+// read (no-op with a private stage).
+__device__ __forceinline__ void stage_release(RowStage &st, const StagePool &sp, int lane) {
+  if (sp.count == 0 || st.slot < 0) return;
+  __syncwarp();
+  if (lane == 0) {
+    // this team's reads of the stage come before any later copy into it
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    *(volatile uint32_t *)(sp.phases + st.slot) = st.phase;
+    __threadfence_block();
+    atomicOr(sp.mask, 1u << st.slot);
+  }
+  st.slot = -1;
+}
 
 // Blocks (8 floats each) of the first half-row of a split stage: the odd
 // tail block (processed first, distance.cpp:42-45) plus the leading blocks.
@@ -360,7 +449,7 @@ __device__ __forceinline__ void stage_issue(const GraphView &g, const WarpSmem &
   __syncwarp();
   if (lane < m) {
     const float *row = g.base + (size_t)cid[lane] * (size_t)(nb * 8);
-    float *dst = s.stage + lane * row_words;
+    float *dst = st.buf + lane * row_words;
     if (nblocks > 0)
       asm volatile(
           "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
@@ -446,8 +535,10 @@ __device__ __forceinline__ float pair_finish(const GraphView &g, int h, float a0
 // when a stage wait timed out.
 template <int NB>
 __device__ __forceinline__ bool eval_staged(const GraphView &g, const WarpSmem &s, RowStage &st,
-                                            const SmemPlan &p, const uint32_t *cid, uint32_t *ckey,
-                                            int nc, bool first_issued, int lane) {
+                                            const StagePool &sp, const SmemPlan &p,
+                                            const uint32_t *cid, uint32_t *ckey, int nc,
+                                            bool first_issued, int lane) {
+  if (!stage_acquire(st, sp, lane)) return false;
   const int srows = (int)p.stage_rows;
   const bool split = p.stage_split > 1;
   const int nb = NB > 0 ? NB : (int)g.nb;
@@ -457,7 +548,7 @@ __device__ __forceinline__ bool eval_staged(const GraphView &g, const WarpSmem &
   const int h = lane & 1, c = lane >> 1;
   for (int p0 = 0; p0 < nc; p0 += srows) {
     const int m = min(srows, nc - p0);
-    const float *row = s.stage + (c < m ? c : 0) * p.stage_row_words;
+    const float *row = st.buf + (c < m ? c : 0) * p.stage_row_words;
     float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
     if (!split) {
       if (p0 > 0 || !first_issued) stage_issue(g, s, st, cid + p0, m, 2, p.stage_row_words, lane);
@@ -476,6 +567,7 @@ __device__ __forceinline__ bool eval_staged(const GraphView &g, const WarpSmem &
     if (h == 0 && c < m) ckey[p0 + c] = float_to_key(d);
     __syncwarp();
   }
+  stage_release(st, sp, lane);
   return true;
 }
 
@@ -645,7 +737,8 @@ template <int NB, int RCH>
 __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qsrc, int K, int L,
                                 uint32_t *out_ids, float *out_dists, uint32_t *out_ndc,
                                 uint32_t *out_hops, int32_t *out_status, const WarpSmem &s,
-                                const SmemPlan &p, RowStage &st, uint32_t max_hops, int lane) {
+                                const SmemPlan &p, RowStage &st, const StagePool &sp,
+                                uint32_t max_hops, int lane) {
   const unsigned lanemask_lt = (1u << lane) - 1u;
   const int qw = (int)g.nb * 8;
   for (int i = lane; i < qw; i += 32) s.q[i] = i < (int)g.dim ? qsrc[i] : 0.f;
@@ -684,7 +777,7 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
       size += __popc(__ballot_sync(kFull, valid));
     }
     __syncwarp();
-    if (!eval_staged<NB>(g, s, st, p, s.cid, s.ckey, size, false, lane)) {
+    if (!eval_staged<NB>(g, s, st, sp, p, s.cid, s.ckey, size, false, lane)) {
       status = kStatusStageTimeout;
       size = 0;
     }
@@ -773,9 +866,11 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
       nc += __popc(fm);
       if (RCH == 1 && nc > 0) {
         __syncwarp();
-        stage_issue(g, s, st, s.cid, min(nc, srows), p.stage_split > 1 ? 0 : 2,
-                    p.stage_row_words, lane);
-        issued = true;
+        if (stage_acquire(st, sp, lane)) {
+          stage_issue(g, s, st, s.cid, min(nc, srows), p.stage_split > 1 ? 0 : 2,
+                      p.stage_row_words, lane);
+          issued = true;
+        }
       }
       qh_record(vis, pr, row[c], fresh, lane);
       __syncwarp();
@@ -789,7 +884,7 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
     __syncwarp();
 
     // 3. distances of the staged rows
-    if (!eval_staged<NB>(g, s, st, p, s.cid, s.ckey, nc, issued, lane)) {
+    if (!eval_staged<NB>(g, s, st, sp, p, s.cid, s.ckey, nc, issued, lane)) {
       status = kStatusStageTimeout;
       break;
     }
@@ -854,16 +949,34 @@ __global__ void __launch_bounds__(256, 2) warp_search_kernel(GraphView g, BatchA
   extern __shared__ __align__(128) uint32_t smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wpb = blockDim.x >> 5;
-  const WarpSmem s = carve_warp(smem + (size_t)warp * p.words_per_team, p);
+  const StagePool sp = carve_pool(smem, p);
+  const WarpSmem s = carve_warp(smem + stage_pool_words(p) + (size_t)warp * p.words_per_team, p);
   RowStage st;
-  st.bar = smem_addr(s.bar);
   st.phase = 0;
   st.broken = false;
-  if (lane == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(st.bar) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  if (p.shared_stages == 0) {  // a private stage, always held
+    st.bar = smem_addr(s.bar);
+    st.buf = s.stage;
+    st.slot = 0;
+    if (lane == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(st.bar) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+  } else {  // the CTA's stage pool
+    st.bar = 0;
+    st.buf = nullptr;
+    st.slot = -1;
+    if (threadIdx.x == 0) {
+      for (uint32_t i = 0; i < sp.count; ++i) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sp.bar0 + 8u * i) : "memory");
+        sp.phases[i] = 0u;
+      }
+      *sp.mask = sp.count >= 32 ? ~0u : ((1u << sp.count) - 1u);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
   }
-  __syncwarp();
   const uint32_t slot = blockIdx.x * wpb + warp;
   const uint32_t nslots = gridDim.x * wpb;
   uint32_t q = slot;
@@ -883,7 +996,7 @@ __global__ void __launch_bounds__(256, 2) warp_search_kernel(GraphView g, BatchA
       warp_search_one<NB, RCH>(g, a.queries + (size_t)q * a.qstride, K, L, a.ids + off,
                                a.dists ? a.dists + off : nullptr, a.ndc ? a.ndc + q : nullptr,
                                a.hops ? a.hops + q : nullptr, a.status ? a.status + q : nullptr, s,
-                               p, st, a.max_hops, lane);
+                               p, st, sp, a.max_hops, lane);
       // a stage copy that never completed leaves this team's stage unusable:
       // wait once more (bounded) for it and take no further queries
       if (st.broken) {
@@ -1817,10 +1930,26 @@ SmemPlan plan_warp_smem(const GraphView &g, int L_max, int hash_cap_override) {
   p.stage_rows = kStageRows;
   while (p.stage_rows > 1 && p.stage_rows * p.stage_row_words * 4u > 65536u) p.stage_rows >>= 1;
   p.stage_words = p.stage_rows * p.stage_row_words;
+  p.shared_stages = 0;
   p.words_per_team = p.stage_words + 4 + p.q_words + 2 * p.pool_cap + 5 * p.cand_cap +
                      (1u << bbits) * 4;
   p.words_per_team = round_up(p.words_per_team, 32);  // 128-byte aligned stages
   return p;
+}
+
+void share_stages(SmemPlan &p, int stages) {
+  const uint32_t rest = p.q_words + 2 * p.pool_cap + 5 * p.cand_cap + (1u << p.hash_log2) * 4;
+  if (stages > 0) {
+    p.shared_stages = (uint32_t)std::min(stages, 32);
+    p.words_per_team = round_up(rest, 32);
+  } else {
+    p.shared_stages = 0;
+    p.words_per_team = round_up(p.stage_words + 4 + rest, 32);
+  }
+}
+
+size_t warp_search_smem_bytes(const SmemPlan &p, int warps_per_block) {
+  return ((size_t)stage_pool_words(p) + (size_t)p.words_per_team * warps_per_block) * 4;
 }
 
 SmemPlan plan_intra_smem(const GraphView &g, int L_max, int width, int hash_cap_override) {
@@ -1901,7 +2030,7 @@ cudaError_t launch_scatter_search(const GraphView &g, const BatchArgs &a, const 
 
 int warp_search_occupancy(const GraphView &g, const SmemPlan &p, int warps_per_block) {
   WarpFn fn = warp_fn(g);
-  const size_t smem = (size_t)p.words_per_team * 4 * warps_per_block;
+  const size_t smem = warp_search_smem_bytes(p, warps_per_block);
   if (allow_max_smem((const void *)fn) != cudaSuccess) return 0;
   int blocks = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, (const void *)fn, warps_per_block * 32,
@@ -1913,7 +2042,7 @@ int warp_search_occupancy(const GraphView &g, const SmemPlan &p, int warps_per_b
 cudaError_t launch_warp_search(const GraphView &g, const BatchArgs &a, const SmemPlan &p,
                                int warps_per_block, int blocks, cudaStream_t stream) {
   WarpFn fn = warp_fn(g);
-  const size_t smem = (size_t)p.words_per_team * 4 * warps_per_block;
+  const size_t smem = warp_search_smem_bytes(p, warps_per_block);
   cudaError_t e = allow_max_smem((const void *)fn);
   if (e != cudaSuccess) return e;
   if (blocks <= 0) blocks = (int)((a.nq + warps_per_block - 1) / warps_per_block);
