@@ -263,15 +263,6 @@ int ss_set_tuning(ss_index *h, int warps_per_block, int hash_cap, int blocks_per
  * leaves room for more teams per SM.  Results never depend on it. */
 int ss_set_shared_stages(ss_index *h, int stages_per_block);
 
-/* Visited table of the batched kernel's persistent launches held in global
- * memory instead of shared memory: `slots` ids per query team (0 = off, or
- * a power of two in [1024, 65536]; about 32 bytes per 8 slots per resident
- * team, L2-resident), probed with one L2 round trip per hop.  A larger table
- * forgets fewer visited ids and so repeats fewer distance evaluations, and
- * it frees the shared memory of the in-block table.  Results never depend
- * on it. */
-int ss_set_visited_cache(ss_index *h, int slots);
-
 /* ---- exact brute force -------------------------------------------------- */
 
 /* Exact k nearest base rows of each query by brute force (no graph needed);

@@ -344,13 +344,12 @@ class ANNSearch:
         return n.value
 
     def set_tuning(self, warps_per_block: int = 0, hash_cap: int = 0, blocks_per_sm_cap: int = 0,
-                   shared_stages: int = 0, visited_cache: int = 0):
-        """Launch layout of the batched kernel (ss_set_tuning,
-        ss_set_shared_stages, ss_set_visited_cache); never changes results."""
+                   shared_stages: int = 0):
+        """Launch layout of the batched kernel (ss_set_tuning and
+        ss_set_shared_stages); never changes results."""
         self._check(self._lib.ss_set_tuning(self._h, int(warps_per_block), int(hash_cap),
                                             int(blocks_per_sm_cap)))
         self._check(self._lib.ss_set_shared_stages(self._h, int(shared_stages)))
-        self._check(self._lib.ss_set_visited_cache(self._h, int(visited_cache)))
 
 
 class SearchPlan:

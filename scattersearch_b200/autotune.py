@@ -25,9 +25,6 @@ DEFAULT_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "scattersearch_b
 WPB_CANDIDATES = (1, 2, 4, 8)
 # (teams per CTA, shared row stages) layouts tried besides one stage per team
 SHARED_CANDIDATES = ((2, 1), (4, 2), (4, 3), (8, 3), (8, 4), (8, 5))
-# global-memory visited tables (slots per team) tried with each layout; the
-# in-block table is then at its minimum, so hash_cap is not swept for them
-VISITED_CACHE_CANDIDATES = (8192, 16384)
 _lock = threading.Lock()
 
 
@@ -87,14 +84,13 @@ def apply(index, L: int, path: str = DEFAULT_CACHE, device=None) -> dict | None:
     choice = load_cache(path).get(key)
     if choice:
         index.set_tuning(int(choice["warps_per_block"]), int(choice["hash_cap"]), 0,
-                         int(choice.get("shared_stages", 0)), int(choice.get("visited_cache", 0)))
+                         int(choice.get("shared_stages", 0)))
     return choice
 
 
 def autotune(index, queries, K: int, L: int, reps: int = 3, path: str | None = DEFAULT_CACHE,
              device=None, wpb_candidates=WPB_CANDIDATES, hash_caps=None, Ks=None, Ls=None,
-             out_off=None, shared_candidates=SHARED_CANDIDATES,
-             visited_caches=VISITED_CACHE_CANDIDATES) -> dict:
+             out_off=None, shared_candidates=SHARED_CANDIDATES) -> dict:
     """Times every (warps_per_block, shared_stages, hash_cap) candidate --
     each of ``wpb_candidates`` with a stage per team, and each pair of
     ``shared_candidates`` -- on ``queries`` (a
@@ -123,36 +119,33 @@ def autotune(index, queries, K: int, L: int, reps: int = 3, path: str | None = D
     ref = None
     table = []
     layouts = [(w, 0) for w in wpb_candidates] + list(shared_candidates or ())
-    configs = [(wpb, stages, hc, 0) for hc in (hash_caps or hash_candidates(L))
-               for wpb, stages in layouts]
-    configs += [(wpb, stages, 0, vc) for vc in (visited_caches or ()) for wpb, stages in layouts]
-    for wpb, stages, hc, vc in configs:
-        index.set_tuning(wpb, hc, 0, stages, vc)
-        launch()
-        stream.synchronize()
-        got = ids.cpu().numpy()
-        if ref is None:
-            ref = got.copy()
-        elif not np.array_equal(got, ref):
-            raise RuntimeError(f"ids differ under warps_per_block={wpb}, "
-                               f"shared_stages={stages}, hash_cap={hc}, visited_cache={vc}")
-        times = []
-        for _ in range(reps):
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(stream)
+    for hc in (hash_caps or hash_candidates(L)):
+        for wpb, stages in layouts:
+            index.set_tuning(wpb, hc, 0, stages)
             launch()
-            b.record(stream)
             stream.synchronize()
-            times.append(a.elapsed_time(b))
-        table.append({"warps_per_block": wpb, "shared_stages": stages, "hash_cap": hc,
-                      "visited_cache": vc, "ms": float(np.median(times))})
+            got = ids.cpu().numpy()
+            if ref is None:
+                ref = got.copy()
+            elif not np.array_equal(got, ref):
+                raise RuntimeError(f"ids differ under warps_per_block={wpb}, "
+                                   f"shared_stages={stages}, hash_cap={hc}")
+            times = []
+            for _ in range(reps):
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                launch()
+                b.record(stream)
+                stream.synchronize()
+                times.append(a.elapsed_time(b))
+            table.append({"warps_per_block": wpb, "shared_stages": stages, "hash_cap": hc,
+                          "ms": float(np.median(times))})
     best = min(table, key=lambda r: r["ms"])
-    index.set_tuning(best["warps_per_block"], best["hash_cap"], 0, best["shared_stages"],
-                     best["visited_cache"])
+    index.set_tuning(best["warps_per_block"], best["hash_cap"], 0, best["shared_stages"])
     choice = {"warps_per_block": best["warps_per_block"], "shared_stages": best["shared_stages"],
-              "hash_cap": best["hash_cap"], "visited_cache": best["visited_cache"],
-              "ms": best["ms"], "sample_queries": nq, "K": "per query" if uneven else K, "L": L}
+              "hash_cap": best["hash_cap"], "ms": best["ms"], "sample_queries": nq,
+              "K": "per query" if uneven else K, "L": L}
     if path:
         save_choice(tuning_key(_gpu_name(device if device is not None else dev),
                                index.dimension, index.rstride, L), choice, path)

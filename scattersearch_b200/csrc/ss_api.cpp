@@ -72,7 +72,7 @@ struct DevBuf {
 struct SearchCtx {
   cudaStream_t stream = nullptr;
   DevBuf q, ids, dists, Ks, Ls, off, counter, status, ndc, hops, spill, bf_q, bf_qpack, bf_cand,
-      bf_err, gvis;
+      bf_err;
   std::vector<int32_t> h_status;
   ~SearchCtx() {
     if (stream) cudaStreamDestroy(stream);
@@ -113,7 +113,6 @@ struct ss_index {
   int hash_cap_override = 0;
   int blocks_per_sm_cap = 0;
   int shared_stages = 0;  // row stages shared by a CTA's teams (0 = one per team)
-  int gvis_slots = 0;     // per-team visited table in global memory (0 = shared memory only)
 
   ssb::GraphView view() const {
     ssb::GraphView g;
@@ -273,25 +272,13 @@ int choose_wpb(ss_index *h, ssb::SmemPlan &p) {
   return best;
 }
 
-// With global visited tables the shared-memory table shrinks to its minimum.
-constexpr int kGvisSmemSlots = 512;
-uint32_t gvis_log2b(const ss_index *h) {
-  uint32_t b = 0;
-  while ((8u << b) < (uint32_t)h->gvis_slots) ++b;
-  return b;
-}
-size_t gvis_bytes(const ss_index *h, int blocks, int wpb) {
-  return (size_t)blocks * wpb * (8u << gvis_log2b(h)) * 4;
-}
-
 // Core batched launch into caller-provided device buffers on `stream`.
 int launch_batch(ss_index *h, SearchCtx *c, const float *d_q, uint32_t nq, const int32_t *d_K,
                  const int32_t *d_L, const int64_t *d_off, int K0, int L0, int L_max,
                  uint32_t *d_ids, float *d_dists, uint32_t *d_ndc, uint32_t *d_hops,
                  cudaStream_t stream, bool persistent) {
   ssb::GraphView g = h->view();
-  const bool gv = persistent && h->gvis_slots > 0;
-  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, gv ? kGvisSmemSlots : h->hash_cap_override);
+  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, h->hash_cap_override);
   const int wpb = choose_wpb(h, plan);
   if (ssb::warp_search_smem_bytes(plan, wpb) > 227 * 1024)
     return set_err(h, SS_ERR_UNSUPPORTED, "L=%d needs %u bytes of shared memory per query",
@@ -317,11 +304,6 @@ int launch_batch(ss_index *h, SearchCtx *c, const float *d_q, uint32_t nq, const
   a.status = c->status.as<int32_t>();
   a.work_counter = persistent ? c->counter.as<uint32_t>() : nullptr;
   a.max_hops = h->n + 1;  // the warp kernel's visited table needs no global memory
-  if (gv) {
-    SS_CUDA(h, c->gvis.ensure(gvis_bytes(h, blocks, wpb)), "visited tables");
-    a.gvis = c->gvis.as<uint4>();
-    a.gvis_log2b = gvis_log2b(h);
-  }
   if (persistent) SS_CUDA(h, cudaMemsetAsync(c->counter.p, 0, 4, stream), "counter reset");
   SS_CUDA(h, cudaMemsetAsync(c->status.p, 0, (size_t)nq * 4, stream), "status reset");
   SS_CUDA(h, ssb::launch_warp_search(g, a, plan, wpb, blocks, stream), "search launch");
@@ -766,7 +748,6 @@ struct ss_plan {
   uint32_t nq = 0;
   int32_t *status = nullptr;
   uint32_t *counter = nullptr;
-  uint4 *gvis = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
 };
@@ -778,7 +759,6 @@ void plan_free(ss_plan *p) {
   if (p->graph) cudaGraphDestroy(p->graph);
   if (p->status) cudaFree(p->status);
   if (p->counter) cudaFree(p->counter);
-  if (p->gvis) cudaFree(p->gvis);
   delete p;
 }
 }  // namespace
@@ -820,24 +800,13 @@ int ss_plan_create_uneven(ss_index *h, const float *queries, uint32_t nq, const 
   // Plan the launch outside the capture (occupancy queries and kernel
   // attributes are not stream work).
   ssb::GraphView g = h->view();
-  const bool gv = h->gvis_slots > 0;
-  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, gv ? kGvisSmemSlots : h->hash_cap_override);
+  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, h->hash_cap_override);
   const int wpb = choose_wpb(h, plan);
   const int blocks = persistent_blocks(h, plan, wpb, nq);
   if (ssb::warp_search_smem_bytes(plan, wpb) > 227 * 1024 || blocks <= 0) {
     plan_free(p);
     cudaStreamDestroy(cs);
     return set_err(h, SS_ERR_UNSUPPORTED, "L=%d cannot be planned on this device", L_max);
-  }
-  if (gv) {
-    e = cudaMalloc(&p->gvis, gvis_bytes(h, blocks, wpb));
-    if (e != cudaSuccess) {
-      p->gvis = nullptr;
-      plan_free(p);
-      cudaStreamDestroy(cs);
-      std::lock_guard<std::mutex> lk(h->mu);
-      return cuda_fail(h, e, "visited tables");
-    }
   }
   ssb::BatchArgs a{};
   a.queries = queries;
@@ -853,10 +822,6 @@ int ss_plan_create_uneven(ss_index *h, const float *queries, uint32_t nq, const 
   a.status = p->status;
   a.work_counter = p->counter;
   a.max_hops = h->n + 1;
-  if (gv) {
-    a.gvis = p->gvis;
-    a.gvis_log2b = gvis_log2b(h);
-  }
   e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
     cudaError_t e1 = cudaMemsetAsync(p->counter, 0, 4, cs);
@@ -1222,15 +1187,6 @@ int ss_set_shared_stages(ss_index *h, int stages_per_block) {
   if (stages_per_block < 0 || stages_per_block > 32)
     return set_err(h, SS_ERR_INVALID_ARGUMENT, "stages_per_block must be in [0, 32]");
   h->shared_stages = stages_per_block;
-  return SS_OK;
-}
-
-int ss_set_visited_cache(ss_index *h, int slots) {
-  if (!h) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null index handle");
-  if (slots != 0 && (slots < 1024 || slots > 65536 || (slots & (slots - 1))))
-    return set_err(h, SS_ERR_INVALID_ARGUMENT,
-                   "visited cache slots must be 0 or a power of two in [1024, 65536]");
-  h->gvis_slots = slots;
   return SS_OK;
 }
 

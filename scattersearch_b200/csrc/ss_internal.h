@@ -37,12 +37,6 @@ struct BatchArgs {
   uint32_t *spill_bits;    // per-slot visited bitsets, spill_words each
   uint32_t spill_words;
   uint32_t max_hops;
-  // warp kernel, persistent launches: per-team visited table in global
-  // memory (L2-resident), 2^gvis_log2b buckets of 8 ids each per team,
-  // indexed by team = blockIdx.x * warps_per_block + warp; null = the
-  // shared-memory table only
-  uint4 *gvis;
-  uint32_t gvis_log2b;
 };
 
 // Per-team shared-memory plan (sizes in 4-byte words, all multiples of 4).

@@ -231,74 +231,6 @@ __device__ __forceinline__ void qh_record(QHash &h, const QProbe &pr, uint32_t i
   if (__any_sync(kFull, ev)) h.lossy = true;
 }
 
-// ---- per-team visited table in global memory (optional) -----------------
-// Buckets of 8 ids (id + 1; 0 = empty), two choices per id, read from L2
-// (ld.global.cg: this warp alone reads and writes its region).  Like the
-// shared-memory table it may forget an id (a full bucket pair overwrites a
-// slot), which only costs a repeated evaluation.
-struct GVis {
-  uint4 *bkt;      // 2 uint4 per bucket
-  uint32_t log2b;  // log2(buckets)
-};
-
-struct GProbe {
-  uint32_t b1, b2;
-  uint4 v1a, v1b, v2a, v2b;
-};
-
-__device__ __forceinline__ uint4 ldcg4(const uint4 *p) {
-  uint4 v;
-  asm volatile("ld.global.cg.v4.u32 {%0, %1, %2, %3}, [%4];"
-               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-               : "l"(p)
-               : "memory");
-  return v;
-}
-
-__device__ __forceinline__ uint32_t eq_mask4(uint4 v, uint32_t k) {
-  return (uint32_t)(v.x == k) | ((uint32_t)(v.y == k) << 1) | ((uint32_t)(v.z == k) << 2) |
-         ((uint32_t)(v.w == k) << 3);
-}
-
-__device__ __forceinline__ bool gv_lookup(const GVis &gv, uint32_t id, GProbe &pr) {
-  pr.b1 = (id * kMix1) >> (32 - gv.log2b);
-  pr.b2 = (id * kMix2) >> (32 - gv.log2b);
-  pr.v1a = ldcg4(gv.bkt + 2 * pr.b1);
-  pr.v1b = ldcg4(gv.bkt + 2 * pr.b1 + 1);
-  pr.v2a = ldcg4(gv.bkt + 2 * pr.b2);
-  pr.v2b = ldcg4(gv.bkt + 2 * pr.b2 + 1);
-  const uint32_t k = id + 1u;
-  return (eq_mask4(pr.v1a, k) | eq_mask4(pr.v1b, k) | eq_mask4(pr.v2a, k) |
-          eq_mask4(pr.v2b, k)) != 0u;
-}
-
-// Records the ids of the `ins` lanes (distinct, not found by gv_lookup):
-// each goes to the emptier of its two buckets; lanes that chose the same
-// bucket take its empty slots in lane order, and a lane left without one
-// overwrites a slot chosen by its id (the table forgets an id).  All 32
-// lanes call it.
-__device__ __forceinline__ void gv_record(const GVis &gv, QHash &h, const GProbe &pr, uint32_t id,
-                                          bool ins, int lane) {
-  const uint32_t e1 = eq_mask4(pr.v1a, 0u) | (eq_mask4(pr.v1b, 0u) << 4);
-  const uint32_t e2 = eq_mask4(pr.v2a, 0u) | (eq_mask4(pr.v2b, 0u) << 4);
-  const bool use1 = __popc(e1) >= __popc(e2);
-  const uint32_t b = use1 ? pr.b1 : pr.b2, e = use1 ? e1 : e2;
-  const unsigned grp = __match_any_sync(kFull, ins ? b : (0x80000000u | (uint32_t)lane));
-  const int r = __popc(grp & ((1u << lane) - 1u));
-  bool ev = false;
-  if (ins) {
-    uint32_t sl;
-    if (r < __popc(e)) {
-      sl = __fns(e, 0, r + 1);
-    } else {
-      sl = (id * kMix3) >> 29;
-      ev = true;
-    }
-    reinterpret_cast<uint32_t *>(gv.bkt)[b * 8 + sl] = id + 1u;
-  }
-  if (__any_sync(kFull, ev)) h.lossy = true;
-}
-
 // Starts an L2 prefetch of the base rows of cid[0..nc) (one bulk prefetch
 // per row, no registers held), so every 16-candidate pass of
 // eval_candidates after the first finds its rows in L2 and the first
@@ -806,16 +738,12 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
                                 uint32_t *out_ids, float *out_dists, uint32_t *out_ndc,
                                 uint32_t *out_hops, int32_t *out_status, const WarpSmem &s,
                                 const SmemPlan &p, RowStage &st, const StagePool &sp,
-                                const GVis &gv, uint32_t max_hops, int lane) {
+                                uint32_t max_hops, int lane) {
   const unsigned lanemask_lt = (1u << lane) - 1u;
   const int qw = (int)g.nb * 8;
   for (int i = lane; i < qw; i += 32) s.q[i] = i < (int)g.dim ? qsrc[i] : 0.f;
   const uint32_t nbk = 1u << p.hash_log2;
   for (uint32_t i = lane; i < nbk; i += 32) s.bkt[i] = make_uint4(~0u, ~0u, ~0u, ~0u);
-  if (gv.bkt) {  // the global table replaces the shared-memory one
-    const uint32_t n4 = 2u << gv.log2b;
-    for (uint32_t i = lane; i < n4; i += 32) gv.bkt[i] = make_uint4(0u, 0u, 0u, 0u);
-  }
   __syncwarp();
 
   QHash vis;
@@ -843,11 +771,8 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
       const bool leader = valid && (peers & lanemask_lt) == 0u;
       if (valid) s.cid[m] = row[c];
       QProbe pr{};
-      GProbe gp{};
-      const bool found =
-          leader && (gv.bkt ? gv_lookup(gv, row[c], gp) : qh_lookup(vis, row[c], pr));
-      if (gv.bkt) gv_record(gv, vis, gp, row[c], leader && !found, lane);
-      else qh_record(vis, pr, row[c], leader && !found, lane);
+      const bool found = leader && qh_lookup(vis, row[c], pr);
+      qh_record(vis, pr, row[c], leader && !found, lane);
       __syncwarp();
       size += __popc(__ballot_sync(kFull, valid));
     }
@@ -935,9 +860,7 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
       const unsigned peers = __match_any_sync(kFull, row[c]);
       const bool leader = valid && (peers & lanemask_lt) == 0u;
       QProbe pr{};
-      GProbe gp{};
-      const bool fresh =
-          leader && !(gv.bkt ? gv_lookup(gv, row[c], gp) : qh_lookup(vis, row[c], pr));
+      const bool fresh = leader && !qh_lookup(vis, row[c], pr);
       const unsigned fm = __ballot_sync(kFull, fresh);
       if (fresh) s.cid[nc + __popc(fm & lanemask_lt)] = row[c];
       nc += __popc(fm);
@@ -949,8 +872,7 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
           issued = true;
         }
       }
-      if (gv.bkt) gv_record(gv, vis, gp, row[c], fresh, lane);
-      else qh_record(vis, pr, row[c], fresh, lane);
+      qh_record(vis, pr, row[c], fresh, lane);
       __syncwarp();
     }
     if (nc == 0) {
@@ -1057,9 +979,6 @@ __global__ void __launch_bounds__(256, 2) warp_search_kernel(GraphView g, BatchA
   }
   const uint32_t slot = blockIdx.x * wpb + warp;
   const uint32_t nslots = gridDim.x * wpb;
-  GVis gv;
-  gv.log2b = a.gvis_log2b;
-  gv.bkt = a.gvis ? a.gvis + (size_t)slot * (2u << a.gvis_log2b) : nullptr;
   uint32_t q = slot;
   for (;;) {
     if (a.work_counter) {
@@ -1077,7 +996,7 @@ __global__ void __launch_bounds__(256, 2) warp_search_kernel(GraphView g, BatchA
       warp_search_one<NB, RCH>(g, a.queries + (size_t)q * a.qstride, K, L, a.ids + off,
                                a.dists ? a.dists + off : nullptr, a.ndc ? a.ndc + q : nullptr,
                                a.hops ? a.hops + q : nullptr, a.status ? a.status + q : nullptr, s,
-                               p, st, sp, gv, a.max_hops, lane);
+                               p, st, sp, a.max_hops, lane);
       // a stage copy that never completed leaves this team's stage unusable:
       // wait once more (bounded) for it and take no further queries
       if (st.broken) {
