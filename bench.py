@@ -523,6 +523,8 @@ def run_ours(args):
     # launch layout (teams per CTA, visited-table size) tuned on a sample
     from scattersearch_b200 import autotune
     tune = autotune.autotune(idx, wl["Q"], K, L, reps=2, path=None)
+    for r in sorted(tune["table"], key=lambda r: r["ms"])[:6]:
+        log(f"  layout {r}")
     log(f"tuned: {tune['warps_per_block']} teams per CTA, {tune['shared_stages']} shared stages "
         f"(0 = one per team), {tune['hash_cap']}-slot visited table")
 
