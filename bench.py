@@ -526,7 +526,7 @@ def run_ours(args):
     for r in sorted(tune["table"], key=lambda r: r["ms"])[:6]:
         log(f"  layout {r}")
     log(f"tuned: {tune['warps_per_block']} teams per CTA, {tune['shared_stages']} shared stages "
-        f"(0 = one per team), {tune['hash_cap']}-slot visited table")
+        f"(0 = one per team) of {tune['stage_rows']} rows, {tune['hash_cap']}-slot visited table")
 
     Qd = wl["Q"]
     ids_d = torch.empty((nq, K), dtype=torch.int32, device=device)
@@ -554,7 +554,8 @@ def run_ours(args):
     ndc = ndc_d.cpu().numpy().astype(np.int64)
     hops = hops_d.cpu().numpy().astype(np.int64)
     ids_exact = ids_d.cpu().numpy().copy()
-    idx.set_tuning(tune["warps_per_block"], tune["hash_cap"], 0, tune["shared_stages"])
+    idx.set_tuning(tune["warps_per_block"], tune["hash_cap"], 0, tune["shared_stages"],
+                   tune["stage_rows"])
     step(with_stats=True)
     torch.cuda.synchronize()
     ndc_dev = ndc_d.cpu().numpy().astype(np.int64)
@@ -626,7 +627,8 @@ def run_ours(args):
 
     online = None if args.no_online else measure_online(idx, wl, L)
     intra = None if args.no_online else measure_intra_latency(idx, wl, L, device)
-    idx.set_tuning(tune["warps_per_block"], tune["hash_cap"], 0, tune["shared_stages"])
+    idx.set_tuning(tune["warps_per_block"], tune["hash_cap"], 0, tune["shared_stages"],
+                   tune["stage_rows"])
 
     peak, peak_kind = measured_hbm_peak()
     traffic, traffic_src = profiled_traffic(args.workload, L, nq)
@@ -648,6 +650,7 @@ def run_ours(args):
                    "ground_truth": wl["gt_info"],
                    "tuning": {"warps_per_block": tune["warps_per_block"],
                               "shared_stages": tune["shared_stages"],
+                              "stage_rows": tune["stage_rows"],
                               "hash_cap": tune["hash_cap"],
                               "sample": f"the {nq} bench queries (launch layout only)"}},
         "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": nq * dim * 4,
@@ -727,7 +730,7 @@ def run_uneven(args):
     tune = autotune.autotune(idx, Qd, total, L_max, reps=2, path=None, Ks=dK, Ls=dL,
                              out_off=doff)
     log(f"tuned: {tune['warps_per_block']} teams per CTA, {tune['shared_stages']} shared stages "
-        f"(0 = one per team), {tune['hash_cap']}-slot visited table")
+        f"(0 = one per team) of {tune['stage_rows']} rows, {tune['hash_cap']}-slot visited table")
     ids_d = torch.empty(total, dtype=torch.int32, device=device)
     dist_d = torch.empty(total, dtype=torch.float32, device=device)
     ndc_d = torch.empty(nq, dtype=torch.int32, device=device)
@@ -746,7 +749,8 @@ def run_uneven(args):
     ndc = ndc_d.cpu().numpy().astype(np.int64)
     hops = hops_d.cpu().numpy().astype(np.int64)
     ids_exact = ids_d.cpu().numpy().copy()
-    idx.set_tuning(tune["warps_per_block"], tune["hash_cap"], 0, tune["shared_stages"])
+    idx.set_tuning(tune["warps_per_block"], tune["hash_cap"], 0, tune["shared_stages"],
+                   tune["stage_rows"])
     stats_pass()
     ndc_dev = ndc_d.cpu().numpy().astype(np.int64)
     if not np.array_equal(ids_d.cpu().numpy(), ids_exact):
@@ -834,6 +838,7 @@ def run_uneven(args):
                    "ground_truth": wl["gt_info"],
                    "tuning": {"warps_per_block": tune["warps_per_block"],
                               "shared_stages": tune["shared_stages"],
+                              "stage_rows": tune["stage_rows"],
                               "hash_cap": tune["hash_cap"]}},
         "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": nq * dim * 4,
                 "d2h_bytes_per_step": total * 8, "ids_equal_device_path": same_ids},

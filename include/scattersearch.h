@@ -256,12 +256,15 @@ int ss_search_scatter_batch_device(ss_index *h, const float *queries, uint32_t n
  * blocks_per_sm_cap: limit on resident CTAs per SM (0 = occupancy limit). */
 int ss_set_tuning(ss_index *h, int warps_per_block, int hash_cap, int blocks_per_sm_cap);
 
-/* Row stages shared by the query teams of one CTA of the batched kernel
- * (0 = each team has its own 16-row stage; n > 0 = a pool of n stages per
- * CTA, used when the CTA has more than n teams).  A team holds a stage only
- * while its rows are copied in and its distances computed, so a shared pool
- * leaves room for more teams per SM.  Results never depend on it. */
-int ss_set_shared_stages(ss_index *h, int stages_per_block);
+/* Row stages of the batched kernel.  stage_rows: base rows one stage holds
+ * (1-16, 0 = 16); a hop with more fresh candidates than that copies and
+ * evaluates them in several passes, and a smaller stage leaves room for more
+ * query teams per SM.  stages_per_block: row stages shared by the query
+ * teams of one CTA (0 = each team has its own; n > 0 = a pool of n stages
+ * per CTA, used when the CTA has more than n teams).  A team holds a stage
+ * only while its rows are copied in and its distances computed.  Results
+ * never depend on either. */
+int ss_set_stage_layout(ss_index *h, int stage_rows, int stages_per_block);
 
 /* ---- exact brute force -------------------------------------------------- */
 

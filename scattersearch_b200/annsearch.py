@@ -344,12 +344,12 @@ class ANNSearch:
         return n.value
 
     def set_tuning(self, warps_per_block: int = 0, hash_cap: int = 0, blocks_per_sm_cap: int = 0,
-                   shared_stages: int = 0):
+                   shared_stages: int = 0, stage_rows: int = 0):
         """Launch layout of the batched kernel (ss_set_tuning and
-        ss_set_shared_stages); never changes results."""
+        ss_set_stage_layout); never changes results."""
         self._check(self._lib.ss_set_tuning(self._h, int(warps_per_block), int(hash_cap),
                                             int(blocks_per_sm_cap)))
-        self._check(self._lib.ss_set_shared_stages(self._h, int(shared_stages)))
+        self._check(self._lib.ss_set_stage_layout(self._h, int(stage_rows), int(shared_stages)))
 
 
 class SearchPlan:

@@ -25,6 +25,8 @@ DEFAULT_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "scattersearch_b
 WPB_CANDIDATES = (1, 2, 4, 8)
 # (teams per CTA, shared row stages) layouts tried besides one stage per team
 SHARED_CANDIDATES = ((2, 1), (4, 2), (4, 3), (8, 3), (8, 4), (8, 5))
+# rows per row stage tried with one stage per team (16 = the default)
+STAGE_ROWS_CANDIDATES = (16, 12)
 _lock = threading.Lock()
 
 
@@ -84,16 +86,18 @@ def apply(index, L: int, path: str = DEFAULT_CACHE, device=None) -> dict | None:
     choice = load_cache(path).get(key)
     if choice:
         index.set_tuning(int(choice["warps_per_block"]), int(choice["hash_cap"]), 0,
-                         int(choice.get("shared_stages", 0)))
+                         int(choice.get("shared_stages", 0)), int(choice.get("stage_rows", 0)))
     return choice
 
 
 def autotune(index, queries, K: int, L: int, reps: int = 3, path: str | None = DEFAULT_CACHE,
              device=None, wpb_candidates=WPB_CANDIDATES, hash_caps=None, Ks=None, Ls=None,
-             out_off=None, shared_candidates=SHARED_CANDIDATES) -> dict:
-    """Times every (warps_per_block, shared_stages, hash_cap) candidate --
-    each of ``wpb_candidates`` with a stage per team, and each pair of
-    ``shared_candidates`` -- on ``queries`` (a
+             out_off=None, shared_candidates=SHARED_CANDIDATES,
+             stage_rows_candidates=STAGE_ROWS_CANDIDATES) -> dict:
+    """Times every (warps_per_block, shared_stages, stage_rows, hash_cap)
+    candidate -- each of ``wpb_candidates`` with a stage per team of each of
+    ``stage_rows_candidates`` rows, and each pair of ``shared_candidates``
+    with 16-row stages -- on ``queries`` (a
     CUDA tensor, nq x dim) and sets the fastest on ``index``.  Raises if two
     candidates return different ids.  Returns the choice with the timing
     table; stores it in the cache at ``path`` (None: no cache).
@@ -118,10 +122,11 @@ def autotune(index, queries, K: int, L: int, reps: int = 3, path: str | None = D
 
     ref = None
     table = []
-    layouts = [(w, 0) for w in wpb_candidates] + list(shared_candidates or ())
+    layouts = [(w, 0, r) for r in (stage_rows_candidates or (16,)) for w in wpb_candidates]
+    layouts += [(w, st, 16) for w, st in (shared_candidates or ())]
     for hc in (hash_caps or hash_candidates(L)):
-        for wpb, stages in layouts:
-            index.set_tuning(wpb, hc, 0, stages)
+        for wpb, stages, rows in layouts:
+            index.set_tuning(wpb, hc, 0, stages, rows)
             launch()
             stream.synchronize()
             got = ids.cpu().numpy()
@@ -129,7 +134,7 @@ def autotune(index, queries, K: int, L: int, reps: int = 3, path: str | None = D
                 ref = got.copy()
             elif not np.array_equal(got, ref):
                 raise RuntimeError(f"ids differ under warps_per_block={wpb}, "
-                                   f"shared_stages={stages}, hash_cap={hc}")
+                                   f"shared_stages={stages}, stage_rows={rows}, hash_cap={hc}")
             times = []
             for _ in range(reps):
                 a = torch.cuda.Event(enable_timing=True)
@@ -139,13 +144,14 @@ def autotune(index, queries, K: int, L: int, reps: int = 3, path: str | None = D
                 b.record(stream)
                 stream.synchronize()
                 times.append(a.elapsed_time(b))
-            table.append({"warps_per_block": wpb, "shared_stages": stages, "hash_cap": hc,
-                          "ms": float(np.median(times))})
+            table.append({"warps_per_block": wpb, "shared_stages": stages, "stage_rows": rows,
+                          "hash_cap": hc, "ms": float(np.median(times))})
     best = min(table, key=lambda r: r["ms"])
-    index.set_tuning(best["warps_per_block"], best["hash_cap"], 0, best["shared_stages"])
+    index.set_tuning(best["warps_per_block"], best["hash_cap"], 0, best["shared_stages"],
+                     best["stage_rows"])
     choice = {"warps_per_block": best["warps_per_block"], "shared_stages": best["shared_stages"],
-              "hash_cap": best["hash_cap"], "ms": best["ms"], "sample_queries": nq,
-              "K": "per query" if uneven else K, "L": L}
+              "stage_rows": best["stage_rows"], "hash_cap": best["hash_cap"], "ms": best["ms"],
+              "sample_queries": nq, "K": "per query" if uneven else K, "L": L}
     if path:
         save_choice(tuning_key(_gpu_name(device if device is not None else dev),
                                index.dimension, index.rstride, L), choice, path)

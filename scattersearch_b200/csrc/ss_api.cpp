@@ -113,6 +113,7 @@ struct ss_index {
   int hash_cap_override = 0;
   int blocks_per_sm_cap = 0;
   int shared_stages = 0;  // row stages shared by a CTA's teams (0 = one per team)
+  int stage_rows = 0;     // rows per row stage (0 = 16)
 
   ssb::GraphView view() const {
     ssb::GraphView g;
@@ -278,7 +279,7 @@ int launch_batch(ss_index *h, SearchCtx *c, const float *d_q, uint32_t nq, const
                  uint32_t *d_ids, float *d_dists, uint32_t *d_ndc, uint32_t *d_hops,
                  cudaStream_t stream, bool persistent) {
   ssb::GraphView g = h->view();
-  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, h->hash_cap_override);
+  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, h->hash_cap_override, h->stage_rows);
   const int wpb = choose_wpb(h, plan);
   if (ssb::warp_search_smem_bytes(plan, wpb) > 227 * 1024)
     return set_err(h, SS_ERR_UNSUPPORTED, "L=%d needs %u bytes of shared memory per query",
@@ -451,7 +452,7 @@ int server_launch(ss_index *h, const float *d_q, uint32_t nq, const int32_t *d_K
                   const int32_t *d_L, const int64_t *d_off, int L_max, uint32_t *d_ids,
                   float *d_dists, int32_t *d_status, uint32_t *d_counter, cudaStream_t stream) {
   ssb::GraphView g = h->view();
-  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, h->hash_cap_override);
+  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, h->hash_cap_override, h->stage_rows);
   const int wpb = choose_wpb(h, plan);
   if (ssb::warp_search_smem_bytes(plan, wpb) > 227 * 1024)
     return set_err(h, SS_ERR_UNSUPPORTED, "L=%d needs %u bytes of shared memory per query",
@@ -800,7 +801,7 @@ int ss_plan_create_uneven(ss_index *h, const float *queries, uint32_t nq, const 
   // Plan the launch outside the capture (occupancy queries and kernel
   // attributes are not stream work).
   ssb::GraphView g = h->view();
-  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, h->hash_cap_override);
+  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, h->hash_cap_override, h->stage_rows);
   const int wpb = choose_wpb(h, plan);
   const int blocks = persistent_blocks(h, plan, wpb, nq);
   if (ssb::warp_search_smem_bytes(plan, wpb) > 227 * 1024 || blocks <= 0) {
@@ -1074,7 +1075,7 @@ int ss_search_batch_noalloc(ss_index *h, const float *queries, uint32_t nq, int 
   DeviceGuard dg(h->device);
   const cudaStream_t st = static_cast<cudaStream_t>(stream);
   ssb::GraphView g = h->view();
-  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L, h->hash_cap_override);
+  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L, h->hash_cap_override, h->stage_rows);
   const int wpb = choose_wpb(h, plan);
   if (ssb::warp_search_smem_bytes(plan, wpb) > 227 * 1024)
     return set_err(h, SS_ERR_UNSUPPORTED, "L=%d needs %u bytes of shared memory per query", L,
@@ -1182,10 +1183,13 @@ int ss_set_tuning(ss_index *h, int warps_per_block, int hash_cap, int blocks_per
   return SS_OK;
 }
 
-int ss_set_shared_stages(ss_index *h, int stages_per_block) {
+int ss_set_stage_layout(ss_index *h, int stage_rows, int stages_per_block) {
   if (!h) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null index handle");
+  if (stage_rows < 0 || stage_rows > 16)
+    return set_err(h, SS_ERR_INVALID_ARGUMENT, "stage_rows must be in [0, 16]");
   if (stages_per_block < 0 || stages_per_block > 32)
     return set_err(h, SS_ERR_INVALID_ARGUMENT, "stages_per_block must be in [0, 32]");
+  h->stage_rows = stage_rows;
   h->shared_stages = stages_per_block;
   return SS_OK;
 }

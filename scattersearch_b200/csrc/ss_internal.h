@@ -68,7 +68,8 @@ enum : int32_t {
 };
 
 // Plans shared memory for a warp-per-query launch.
-SmemPlan plan_warp_smem(const GraphView &g, int L_max, int hash_cap_override);
+// stage_rows: rows of the row stage (0 = 16, the most one pass computes).
+SmemPlan plan_warp_smem(const GraphView &g, int L_max, int hash_cap_override, int stage_rows = 0);
 // Lets the teams of a CTA share `stages` row stages (0: a private stage per
 // team); updates words_per_team.
 void share_stages(SmemPlan &p, int stages);

@@ -1897,7 +1897,7 @@ uint32_t log2_of(uint32_t p) {
 
 }  // namespace
 
-SmemPlan plan_warp_smem(const GraphView &g, int L_max, int hash_cap_override) {
+SmemPlan plan_warp_smem(const GraphView &g, int L_max, int hash_cap_override, int stage_rows) {
   SmemPlan p{};
   p.q_words = g.nb * 8;
   p.pool_cap = round_up((uint32_t)L_max, 32);
@@ -1925,9 +1925,10 @@ SmemPlan plan_warp_smem(const GraphView &g, int L_max, int hash_cap_override) {
   // the cost of one L2 round trip per pass (measured slower than whole rows
   // at 200 dims: 546k against 640k queries/s at L = 400), and fewer rows
   // only beyond that.
-  p.stage_split = kStageRows * g.nb * 32u > 65536u ? 2 : 1;
+  const uint32_t rows = stage_rows > 0 ? (uint32_t)std::min(stage_rows, kStageRows) : kStageRows;
+  p.stage_split = rows * g.nb * 32u > 65536u ? 2 : 1;
   p.stage_row_words = (p.stage_split > 1 ? split_first(g.nb) : g.nb) * 8;
-  p.stage_rows = kStageRows;
+  p.stage_rows = rows;
   while (p.stage_rows > 1 && p.stage_rows * p.stage_row_words * 4u > 65536u) p.stage_rows >>= 1;
   p.stage_words = p.stage_rows * p.stage_row_words;
   p.shared_stages = 0;

@@ -61,10 +61,11 @@ def test_batched_equals_plain(oracle_lib, name):
         assert _same_bits(d, o_d)
         # launch layouts: teams per CTA, with a stage per team or a shared
         # pool of fewer stages (a single shared stage included)
-        for wpb, stages in ((1, 0), (2, 0), (8, 0), (4, 1), (8, 3), (8, 6)):
-            idx.set_tuning(warps_per_block=wpb, shared_stages=stages)
+        for wpb, stages, rows in ((1, 0, 0), (2, 0, 0), (8, 0, 0), (4, 1, 0), (8, 3, 0),
+                                  (8, 6, 0), (1, 0, 12), (2, 0, 5), (4, 2, 1)):
+            idx.set_tuning(warps_per_block=wpb, shared_stages=stages, stage_rows=rows)
             ids2, d2 = idx.search_batch(fx["queries"], K, L)
-            assert np.array_equal(ids2, ids) and _same_bits(d2, d), (wpb, stages)
+            assert np.array_equal(ids2, ids) and _same_bits(d2, d), (wpb, stages, rows)
         idx.set_tuning()
     idx.close()
 
@@ -338,8 +339,8 @@ def test_autotuner_keeps_results_and_caches_its_choice(oracle_lib, tmp_path):
     path = str(tmp_path / "tuning.json")
     choice = autotune.autotune(idx, q, 10, 100, reps=1, path=path)
     assert choice["warps_per_block"] in (1, 2, 4, 8) and choice["hash_cap"] >= 1024
-    assert len(choice["table"]) == (4 + len(autotune.SHARED_CANDIDATES)) * len(
-        autotune.hash_candidates(100))
+    assert len(choice["table"]) == (4 * len(autotune.STAGE_ROWS_CANDIDATES) + len(
+        autotune.SHARED_CANDIDATES)) * len(autotune.hash_candidates(100))
     after, _ = idx.search_batch(fx["queries"], 10, 100)
     assert np.array_equal(before, after)
     idx.set_tuning()
@@ -366,7 +367,7 @@ def test_graph_captured_uneven_plan(oracle_lib):
     from scattersearch_b200 import autotune
     choice = autotune.autotune(idx, q, total, 512, reps=1, path=None, Ks=dK, Ls=dL,
                                out_off=doff, wpb_candidates=(2, 8), hash_caps=(1024, 4096),
-                               shared_candidates=((8, 3),))
+                               shared_candidates=((8, 3),), stage_rows_candidates=(16,))
     assert len(choice["table"]) == 6
     plan = idx.plan_batch_uneven_device(q, nq, dK, dL, doff, 512, ids, d)
     o_ids, o_d, _, _ = oracle_lib.search(fx["base"], fx["adj"], int(fx["ep"]), 0, Q, Ks=Ks, Ls=Ls)
