@@ -172,3 +172,48 @@ def test_autotune_keys_and_cache(tmp_path):
     at.save_choice("other", {"warps_per_block": 1, "hash_cap": 1024}, path)
     data = at.load_cache(path)
     assert data[k1]["hash_cap"] == 2048 and set(data) == {k1, "other"}
+
+
+def test_autotune_apply_restores_the_whole_layout(tmp_path, monkeypatch):
+    """A cached choice sets teams per CTA, table size, stage rows and shared
+    stages on the index (a stand-in that records the call; no GPU)."""
+    from scattersearch_b200 import autotune as at
+    monkeypatch.setattr(at, "_gpu_name", lambda device=None: "GPU-X")
+
+    class FakeIndex:
+        dimension, rstride = 96, 32
+        calls = []
+
+        def set_tuning(self, *args):
+            self.calls.append(args)
+
+    path = str(tmp_path / "tuning.json")
+    idx = FakeIndex()
+    assert at.apply(idx, 300, path=path) is None and idx.calls == []
+    at.save_choice(at.tuning_key("GPU-X", 96, 32, 300),
+                   {"warps_per_block": 4, "hash_cap": 2048, "shared_stages": 3,
+                    "stage_rows": 12}, path)
+    assert at.apply(idx, 400, path=path)["hash_cap"] == 2048  # same L bucket (512)
+    assert idx.calls == [(4, 2048, 0, 3, 12)]
+    # choices cached before stage layouts existed still apply
+    at.save_choice(at.tuning_key("GPU-X", 96, 32, 40), {"warps_per_block": 1, "hash_cap": 1024},
+                   path)
+    at.apply(idx, 40, path=path)
+    assert idx.calls[-1] == (1, 1024, 0, 0, 0)
+    assert len(at.SHARED_CANDIDATES) and all(s < w for w, s in at.SHARED_CANDIDATES)
+
+
+def test_uneven_recall_helper():
+    """Config 4's recall: recall@10 over queries with K >= 10 (their first ten
+    ids) and recall@1 over queries with K = 1."""
+    import bench
+    Ks = np.array([1, 10, 100, 1], np.int32)
+    off = np.concatenate([[0], np.cumsum(Ks)[:-1]])
+    gt = np.array([np.arange(10) + 100 * i for i in range(4)])
+    ids = np.zeros(int(Ks.sum()), np.uint32)
+    ids[off[0]] = 0                                # K=1, hit
+    ids[off[1]:off[1] + 10] = np.arange(100, 110)  # K=10, all ten
+    ids[off[2]:off[2] + 10] = np.r_[200:205, 900:905]  # K=100, five of ten in its first ten
+    ids[off[3]] = 999                              # K=1, miss
+    r10, r1, n10, n1 = bench.recall_uneven(ids, off, Ks, gt)
+    assert (n10, n1) == (2, 2) and r10 == 0.75 and r1 == 0.5
