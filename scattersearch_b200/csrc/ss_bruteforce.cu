@@ -41,6 +41,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+#include <set>
+#include <utility>
+
 #include "ss_distance.cuh"
 #include "ss_internal.h"
 
@@ -491,11 +495,30 @@ __global__ void bf_norms_kernel(const float *base, uint32_t n, uint32_t pitch, f
   if (lane == 0) out[warp] = s;
 }
 
+// Raises a kernel's dynamic shared-memory limit to the device's opt-in
+// maximum, once per (device, kernel).  One fixed value for every launch: a
+// per-launch size set from several host threads could race with another
+// thread's launch of the same kernel.
+cudaError_t allow_max_smem_bf(const void *fn) {
+  static std::mutex mu;
+  static std::set<std::pair<int, const void *>> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count({dev, fn})) return cudaSuccess;
+  int optin = 0;
+  e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+  if (e == cudaSuccess) done.insert({dev, fn});
+  return e;
+}
+
 template <int C>
 cudaError_t launch_candidates(const BruteArgs &a, cudaStream_t s) {
   static_assert(kTcSmem <= 227 * 1024, "candidate kernel exceeds shared memory");
-  cudaError_t e = cudaFuncSetAttribute((const void *)bf_tc_candidates_kernel<C>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+  cudaError_t e = allow_max_smem_bf((const void *)bf_tc_candidates_kernel<C>);
   if (e != cudaSuccess) return e;
   dim3 grid((a.nq + kTM - 1) / kTM, a.splits);
   bf_tc_candidates_kernel<C><<<grid, kTcThreads, kTcSmem, s>>>(a);
@@ -505,8 +528,7 @@ cudaError_t launch_candidates(const BruteArgs &a, cudaStream_t s) {
 template <int C, int SC>
 cudaError_t launch_rerank(const BruteArgs &a, const GraphView &g, cudaStream_t s) {
   const size_t smem = (size_t)4 * a.nb * 8 * 4 + (size_t)4 * 2 * C * 4;
-  cudaError_t e = cudaFuncSetAttribute((const void *)bf_rerank_kernel<C, SC>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = allow_max_smem_bf((const void *)bf_rerank_kernel<C, SC>);
   if (e != cudaSuccess) return e;
   bf_rerank_kernel<C, SC><<<(a.nq + 3) / 4, 128, smem, s>>>(a, g);
   return cudaGetLastError();

@@ -98,3 +98,31 @@ def test_graph_knn_from_the_brute_force(oracle_lib):
     assert ids[100][0] == 7 and d[100][0] == 0.0
     adj, ep = graph.build_graph(X, R=16, knn_k=k, device="cuda", knn_backend="bruteforce")
     assert adj.shape == (6000, 16) and 0 <= ep < 6000
+
+
+def test_bruteforce_from_several_threads(oracle_lib):
+    """Concurrent callers on one index (each call takes its own context and
+    stream) get the single-caller results."""
+    import threading
+    fx = load_fixture("search_ip_d96")
+    idx = _index(fx["base"], int(fx["metric"]))
+    Q = fx["queries"]
+    want = {k: idx.bruteforce(Q, k) for k in (8, 40, 100)}
+    errors = []
+
+    def worker(k):
+        try:
+            for _ in range(3):
+                ids, d = idx.bruteforce(Q, k)
+                if not (np.array_equal(ids, want[k][0]) and _same_bits(d, want[k][1])):
+                    errors.append(k)
+        except Exception as e:  # pragma: no cover - reported below
+            errors.append(repr(e))
+
+    th = [threading.Thread(target=worker, args=(k,)) for k in (8, 40, 100, 40)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert not errors
+    idx.close()
