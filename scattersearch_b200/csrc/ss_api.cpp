@@ -107,6 +107,12 @@ struct ss_index {
   std::mutex norm_mu;
   DevBuf xnorm, bpack;
   bool have_norms = false, have_bpack = false;
+  // recorded after the kernels that built them; later brute-force calls on
+  // any stream wait for it
+  cudaEvent_t bf_ready = nullptr;
+  ~ss_index() {
+    if (bf_ready) cudaEventDestroy(bf_ready);
+  }
 
   // launch tuning (set by the autotuner through ss_set_tuning); 0 = automatic
   int warps_per_block = 0;
@@ -877,29 +883,35 @@ int bruteforce_common(ss_index *h, SearchCtx *c, const float *d_queries, size_t 
                       uint32_t nq, int k, uint32_t *d_ids, float *d_dists, cudaStream_t stream) {
   const uint32_t pitch = h->nb * 8;
   const float *xnorm = nullptr;
-  if (h->metric == SS_METRIC_L2) {
+  const float *bpack = nullptr;
+  {
+    // the norms and the packed base are built once, on the first caller's
+    // stream; every later caller's stream waits for that work
     std::lock_guard<std::mutex> lk(h->norm_mu);
-    if (!h->have_norms) {
+    bool built = false;
+    if (h->metric == SS_METRIC_L2 && !h->have_norms) {
       SS_CUDA(h, h->xnorm.ensure((size_t)h->n * 4), "norm buffer");
       SS_CUDA(h, ssb::launch_norms(h->base.as<float>(), h->n, pitch, h->xnorm.as<float>(), stream),
               "norm launch");
       h->have_norms = true;
+      built = true;
     }
-    xnorm = h->xnorm.as<float>();
-  }
-  ssb::BrutePlan bp = ssb::plan_bruteforce(h->n, nq, k, h->sm_count);
-  const float *bpack = nullptr;
-  {
-    std::lock_guard<std::mutex> lk(h->norm_mu);
     if (!h->have_bpack) {
       SS_CUDA(h, h->bpack.ensure(ssb::bruteforce_pack_bytes(h->n, h->dim, true)), "packed base");
       SS_CUDA(h, ssb::launch_pack(h->base.as<float>(), h->n, pitch, h->dim, true,
                                   h->bpack.as<float>(), stream),
               "base packing");
       h->have_bpack = true;
+      built = true;
     }
+    if (!h->bf_ready)
+      SS_CUDA(h, cudaEventCreateWithFlags(&h->bf_ready, cudaEventDisableTiming), "event");
+    if (built) SS_CUDA(h, cudaEventRecord(h->bf_ready, stream), "event record");
+    else SS_CUDA(h, cudaStreamWaitEvent(stream, h->bf_ready, 0), "event wait");
+    if (h->metric == SS_METRIC_L2) xnorm = h->xnorm.as<float>();
     bpack = h->bpack.as<float>();
   }
+  ssb::BrutePlan bp = ssb::plan_bruteforce(h->n, nq, k, h->sm_count);
   const uint32_t lists = 2 * bp.splits;
   SS_CUDA(h, c->bf_q.ensure((size_t)nq * pitch * 4), "query buffer");
   SS_CUDA(h, c->bf_qpack.ensure(ssb::bruteforce_pack_bytes(nq, h->dim, false)), "packed queries");

@@ -102,12 +102,15 @@ def test_graph_knn_from_the_brute_force(oracle_lib):
 
 def test_bruteforce_from_several_threads(oracle_lib):
     """Concurrent callers on one index (each call takes its own context and
-    stream) get the single-caller results."""
+    stream) get the single-caller results, also when their first calls race
+    to build the index's packed base and norms."""
     import threading
-    fx = load_fixture("search_ip_d96")
-    idx = _index(fx["base"], int(fx["metric"]))
+    fx = load_fixture("search_l2_d200")
+    ref = _index(fx["base"], int(fx["metric"]))
     Q = fx["queries"]
-    want = {k: idx.bruteforce(Q, k) for k in (8, 40, 100)}
+    want = {k: ref.bruteforce(Q, k) for k in (8, 40, 100)}
+    ref.close()
+    idx = _index(fx["base"], int(fx["metric"]))  # nothing built yet
     errors = []
 
     def worker(k):
