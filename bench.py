@@ -121,7 +121,10 @@ class Dist:
 
 
 class ClockSampler:
-    """nvidia-smi samples (200 ms) while the timed region runs."""
+    """nvidia-smi samples every 50 ms while the GPU runs the warm-up and timed
+    steps (a timed region of a few 16 ms steps is shorter than nvidia-smi's
+    usual interval, so sampling starts before the warm-up, and the samples
+    taken before it are dropped)."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -130,33 +133,58 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.skip = 0
+
+    def _lines(self):
+        try:
+            with open(self.path) as f:
+                return f.read().splitlines()
+        except OSError:
+            return []
 
     def start(self):
+        """Starts sampling and returns once the first sample is written (at
+        most 3 s), so that the steps that follow are covered."""
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+            return
+        t0 = time.time()
+        while time.time() - t0 < 3.0 and not self._lines():
+            time.sleep(0.01)
+        self.skip = len(self._lines())
+
+    def _one_shot(self):
+        try:
+            out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                  "--format=csv,noheader,nounits"], capture_output=True,
+                                 text=True, timeout=10).stdout
+            return out.splitlines()
+        except (OSError, subprocess.SubprocessError):
+            return []
 
     def stop(self):
         if self.proc is None:
             return None
-        time.sleep(0.25)
+        time.sleep(0.06)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
-        rows = []
-        for line in open(self.path):
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 9:
-                rows.append(parts)
+        lines = self._lines()[self.skip:]
         os.unlink(self.path)
+        window = "warm-up and timed steps"
+        if not lines:  # no sample landed inside the steps: read once right after them
+            lines, window = self._one_shot(), "right after the timed steps"
+        rows = [[p.strip() for p in line.split(",")] for line in lines]
+        rows = [r for r in rows if len(r) >= 9]
         if not rows:
             return None
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
@@ -166,7 +194,7 @@ class ClockSampler:
                           and "Not" not in r[5 + i]})
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(rows), "window": window}
 
 
 PROFILED_TRAFFIC = {
@@ -568,12 +596,12 @@ def run_ours(args):
     device_bytes_per_step = float(ndc_dev.sum() * row_bytes + hops.sum() * 4 * rstride
                                   + nq * 4 * dim)
 
+    sampler = ClockSampler(d.local_rank)
+    sampler.start()
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
     d.barrier()
-    sampler = ClockSampler(d.local_rank)
-    sampler.start()
     torch.cuda.nvtx.range_push("timed")
     evs = []
     for _ in range(args.steps):
@@ -759,12 +787,12 @@ def run_uneven(args):
     rstride = idx.rstride
     bytes_per_step = float(ndc.sum() * 4 * dim + hops.sum() * 4 * rstride + nq * 4 * dim)
 
+    sampler = ClockSampler(d.local_rank)
+    sampler.start()
     for _ in range(args.warmup):
         plan.launch(stream.cuda_stream)
     torch.cuda.synchronize()
     d.barrier()
-    sampler = ClockSampler(d.local_rank)
-    sampler.start()
     evs = []
     for _ in range(args.steps):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
