@@ -217,3 +217,34 @@ def test_uneven_recall_helper():
     ids[off[3]] = 999                              # K=1, miss
     r10, r1, n10, n1 = bench.recall_uneven(ids, off, Ks, gt)
     assert (n10, n1) == (2, 2) and r10 == 0.75 and r1 == 0.5
+
+
+def test_data_tools_split_and_convert(tmp_path):
+    """split_fbin keeps the last vectors as queries (scripts/splitfbin.py);
+    ann_benchmarks_to_fbin writes base/query/ground truth that the readers
+    (and the C ABI loaders' formats) take back unchanged."""
+    from scattersearch_b200 import io as sio
+    rng = np.random.default_rng(2)
+    X = rng.standard_normal((1037, 24)).astype(np.float32)
+    src = str(tmp_path / "all.fbin")
+    sio.write_fbin(src, X)
+    nb, nq, d = sio.split_fbin(src, 37, str(tmp_path / "b.fbin"), str(tmp_path / "q.fbin"))
+    assert (nb, nq, d) == (1000, 37, 24)
+    assert np.array_equal(sio.load_fbin(str(tmp_path / "b.fbin")), X[:1000])
+    assert np.array_equal(sio.load_fbin(str(tmp_path / "q.fbin")), X[1000:])
+    with pytest.raises(ValueError):
+        sio.split_fbin(src, 2000, str(tmp_path / "x.fbin"), str(tmp_path / "y.fbin"))
+    # command line form
+    assert sio.main(["split-fbin", src, "--num-queries", "10", "--base-out",
+                     str(tmp_path / "b2.fbin"), "--query-out", str(tmp_path / "q2.fbin")]) == 0
+    assert sio.load_fbin(str(tmp_path / "q2.fbin")).shape == (10, 24)
+    train = rng.standard_normal((500, 16))          # float64, as some HDF5 sets store
+    test = rng.standard_normal((20, 16))
+    nbr = rng.integers(0, 500, size=(20, 100))
+    paths = [str(tmp_path / n) for n in ("base.fbin", "query.fbin", "gt.bin")]
+    sio.ann_benchmarks_to_fbin(train, test, nbr, *paths, k=10)
+    assert np.array_equal(sio.load_fbin(paths[0]), train.astype(np.float32))
+    assert np.array_equal(sio.load_fbin(paths[1]), test.astype(np.float32))
+    assert np.array_equal(sio.load_groundtruth(paths[2]), nbr[:, :10].astype(np.uint32))
+    with pytest.raises(ValueError):
+        sio.ann_benchmarks_to_fbin(train, test, nbr + 500, *paths)
