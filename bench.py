@@ -469,7 +469,7 @@ def measure_online(idx, wl, L, rates=(100_000, 300_000, 550_000), seconds=0.15):
             "latency": "arrival to result on the host", "rates": out}
 
 
-def measure_intra_latency(idx, wl, L, device, batches=(1, 4, 16), widths=(4, 8), reps=10):
+def measure_intra_latency(idx, wl, L, device, batches=(1, 4, 16), widths=(4, 8, 16), reps=10):
     """Device time of one small batch: the plain kernel (one warp per query)
     and the intra-query kernel (one CTA of W warps per query, W candidates
     expanded per step), with recall@10 of each."""

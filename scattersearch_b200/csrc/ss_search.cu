@@ -1316,36 +1316,46 @@ __global__ void __launch_bounds__(512) intra_search_kernel(GraphView g, BatchArg
     for (int w = 0; w < np; ++w) total += s.wn[w];
     if (total == 0) continue;
 
-    // E. rank merge into the other buffer
+    // E. rank merge into the other buffer.  New entries first, all (list w,
+    //    element e) pairs in parallel: the rank r of each among the new keys
+    //    (ties: lower w, then lower e) and its slot r + (old entries <= key).
+    //    The new keys, in rank order, go to wc_key (free again at this
+    //    point), so each old entry then finds its shift -- the new keys
+    //    strictly below it -- with one search.
     uint32_t *npk = s.pk[cur ^ 1], *npid = s.pid[cur ^ 1];
+    uint32_t *allnew = s.wc_key;  // W * cand_cap >= total entries
     if (threadIdx.x == 0) s.misc[W + 1] = 0x7FFFFFFF;
     __syncthreads();
     int local_min = 0x7FFFFFFF;
-    // old entries
+    for (int t = threadIdx.x; t < total; t += nthr) {
+      int w = 0, e = t;
+      while (e >= s.wn[w]) {
+        e -= s.wn[w];
+        ++w;
+      }
+      const uint32_t key = s.ws_key[w * cc + e];
+      int r = e;
+      for (int v = 0; v < np; ++v) {
+        if (v == w) continue;
+        r += (v < w) ? count_le(s.ws_key + v * cc, s.wn[v], key)
+                     : count_lt(s.ws_key + v * cc, s.wn[v], key);
+      }
+      allnew[r] = key;
+      const int pos = r + count_le(pk, size, key);
+      if (pos < L) {
+        npk[pos] = key;
+        npid[pos] = s.ws_id[w * cc + e];
+      }
+      local_min = min(local_min, pos);
+    }
+    __syncthreads();
+    // old entries, after the new keys strictly below them
     for (int j = threadIdx.x; j < size; j += nthr) {
       const uint32_t key = pk[j];
-      int t = j;
-      for (int w = 0; w < np; ++w) t += count_lt(s.ws_key + w * cc, s.wn[w], key);
-      if (t < L) {
-        npk[t] = key;
-        npid[t] = pid[j];
-      }
-    }
-    // new entries: list w, element e
-    for (int w = 0; w < np; ++w) {
-      for (int e = threadIdx.x; e < s.wn[w]; e += nthr) {
-        const uint32_t key = s.ws_key[w * cc + e];
-        int t = e + count_le(pk, size, key);
-        for (int v = 0; v < np; ++v) {
-          if (v == w) continue;
-          t += (v < w) ? count_le(s.ws_key + v * cc, s.wn[v], key)
-                       : count_lt(s.ws_key + v * cc, s.wn[v], key);
-        }
-        if (t < L) {
-          npk[t] = key;
-          npid[t] = s.ws_id[w * cc + e];
-        }
-        local_min = min(local_min, t);
+      const int pos = j + count_lt(allnew, total, key);
+      if (pos < L) {
+        npk[pos] = key;
+        npid[pos] = pid[j];
       }
     }
     if (local_min != 0x7FFFFFFF) atomicMin(&s.misc[W + 1], local_min);
