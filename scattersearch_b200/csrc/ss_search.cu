@@ -1343,8 +1343,11 @@ __global__ void __launch_bounds__(512) intra_search_kernel(GraphView g, BatchArg
       allnew[r] = key;
       const int pos = r + count_le(pk, size, key);
       if (pos < L) {
+        const uint32_t nid = s.ws_id[w * cc + e];
         npk[pos] = key;
-        npid[pos] = s.ws_id[w * cc + e];
+        npid[pos] = nid;
+        // a new entry near the head is a likely pick of the next step
+        if (pos < cursor + W) prefetch_adj_l2(g, nid);
       }
       local_min = min(local_min, pos);
     }
