@@ -912,7 +912,7 @@ int bruteforce_common(ss_index *h, SearchCtx *c, const float *d_queries, size_t 
     bpack = h->bpack.as<float>();
   }
   ssb::BrutePlan bp = ssb::plan_bruteforce(h->n, nq, k, h->sm_count);
-  const uint32_t lists = 2 * bp.splits;
+  const uint32_t lists = bp.lists;
   SS_CUDA(h, c->bf_q.ensure((size_t)nq * pitch * 4), "query buffer");
   SS_CUDA(h, c->bf_qpack.ensure(ssb::bruteforce_pack_bytes(nq, h->dim, false)), "packed queries");
   SS_CUDA(h, c->bf_cand.ensure((size_t)nq * lists * bp.list_cap * 8), "candidate buffer");

@@ -17,9 +17,10 @@
 //                         mbarrier completion); one thread of warp 1 issues
 //                         tcgen05.mma kind::tf32 in three terms
 //                         (lo*hi + hi*lo + hi*hi, FP32 accumulate) into one
-//                         of two 128 x 256 TMEM accumulators; warps 2-9 read
+//                         of two 128 x 256 TMEM accumulators; warps 2-17 read
 //                         the other accumulator with tcgen05.ld (one query
-//                         row per thread) and keep each query's C best
+//                         row per thread, a quarter of the columns per
+//                         warp) and keep each query's C best
 //                         (approximate score, id) in a candidate list, while
 //                         the tensor core fills the next tile.
 //   bf_rerank_kernel      one warp per query merges the splits' lists, keeps
@@ -58,7 +59,8 @@ constexpr int kStages = 2;
 constexpr uint32_t kABlock = kTM * 128;  // bytes of one hi (or lo) k-block of queries
 constexpr uint32_t kBBlock = kTN * 128;  // bytes of one hi (or lo) k-block of base rows
 constexpr uint32_t kStageBytes = 2 * kABlock + 2 * kBBlock;
-constexpr int kEpiWarps = 8;
+constexpr int kEpiWarps = 16;                // selection warps: 4 per TMEM lane quadrant
+constexpr int kColParts = kEpiWarps / 4;     // column parts of a tile, one list each
 constexpr int kTcThreads = 64 + 32 * kEpiWarps;
 constexpr uint32_t kTmemCols = 2 * kTN;  // two accumulators
 constexpr uint32_t kBarBytes = 8 * (2 * kStages + 5);
@@ -341,14 +343,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) bf_tc_candidates_kernel(BruteAr
       if (!mbar_wait(done_bar, 0)) *broken = 1;
     }
   } else {
-    // ---- selection: 8 warps; warp w reads TMEM lanes 32*(w%4).. (its
-    // queries) and half (w-2)/4 of each tile's columns
-    const int quad = warp & 3, half = (warp - 2) >> 2;
+    // ---- selection: 16 warps; warp w reads TMEM lanes 32*(w%4).. (its
+    // queries) and part (w-2)/4 of each tile's columns
+    const int quad = warp & 3, half = (warp - 2) >> 2;  // half: the column part
     const uint32_t row = quad * 32 + lane;
     const uint32_t q = qt * kTM + row;
     const bool qv = q < a.nq;
     uint64_t *list =
-        a.cand + ((size_t)(qv ? q : 0) * a.lists + split * 2 + half) * (size_t)a.list_stride;
+        a.cand + ((size_t)(qv ? q : 0) * a.lists + split * kColParts + half) *
+                     (size_t)a.list_stride;
     uint64_t thr = kInvalidKey;
     float thr_f = __int_as_float(0x7f800000);  // +inf
     int cnt = 0;
@@ -359,14 +362,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) bf_tc_candidates_kernel(BruteAr
       ok = __all_sync(kFull, mbar_wait(tfull_bar(b), (t >> 1) & 1));
       if (!ok) break;
       tc_fence_after();
-      const uint32_t taddr = tmem + lane_base + b * kTN + half * (kTN / 2);
-      const uint32_t cbase = row_lo + t * kTN + half * (kTN / 2);
+      const uint32_t taddr = tmem + lane_base + b * kTN + half * (kTN / kColParts);
+      const uint32_t cbase = row_lo + t * kTN + half * (kTN / kColParts);
 #pragma unroll 1
-      for (int ch = 0; ch < kTN / 64; ++ch) {
+      for (int ch = 0; ch < kTN / kColParts / 32; ++ch) {
         uint32_t r[32];
         tmem_ld32(taddr + ch * 32, r);
         tmem_wait_ld();
-        if (ch == kTN / 64 - 1) {  // this thread's last read of accumulator b
+        if (ch == kTN / kColParts / 32 - 1) {  // this thread's last read of accumulator b
           tc_fence_before();
           mbar_arrive(tempty_bar(b));
         }
@@ -406,7 +409,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) bf_tc_candidates_kernel(BruteAr
     if (!ok) {
       *broken = 1;
     } else {
-      // each query's C best of this split half, sorted, at the list front
+      // each query's C best of this split's column part, sorted, at the list front
       unsigned have = __ballot_sync(kFull, qv);
       while (have) {
         const int l = __ffs(have) - 1;
@@ -553,13 +556,15 @@ BrutePlan plan_bruteforce(uint32_t n, uint32_t nq, int k, int sm_count) {
   p.C = k + 16 <= 32 ? 32 : (k + 16 <= 64 ? 64 : 128);
   p.list_cap = p.C + 64 <= 128 ? 128 : 256;
   const uint32_t tiles = (nq + kTM - 1) / kTM;
-  // two lists per split (one per column half); at most 1024 candidates to merge
-  const uint32_t max_splits = 512u / (uint32_t)p.C;
+  // kColParts lists per split (one per column part); at most 1024 candidates
+  // to merge
+  const uint32_t max_splits = 1024u / kColParts / (uint32_t)p.C;
   uint32_t splits = 1;
   while (splits < max_splits && tiles * splits < 4u * (uint32_t)sm_count) splits <<= 1;
   // never more splits than 256-row tiles of the base
   while (splits > 1 && (uint64_t)splits * kTN > n) splits >>= 1;
   p.splits = splits;
+  p.lists = kColParts * splits;
   uint32_t rps = (n + splits - 1) / splits;
   p.rows_per_split = (rps + kTN - 1) / kTN * kTN;
   p.kblocks = 0;

@@ -128,7 +128,7 @@ struct BruteArgs {
   int metric;
   int k, C;               // results per query; candidates kept per list (32/64/128)
   uint32_t splits, rows_per_split;
-  uint32_t lists, list_stride;  // candidate lists per query (2 per split); entries per list
+  uint32_t lists, list_stride;  // candidate lists per query (BrutePlan::lists); entries per list
   uint64_t *cand;         // nq x lists x list_stride scratch
   uint32_t *ids;          // nq x k
   float *dists;           // nq x k, may be null
@@ -138,6 +138,7 @@ struct BrutePlan {
   int C;
   uint32_t list_cap;      // entries per candidate list
   uint32_t splits, rows_per_split;
+  uint32_t lists;         // candidate lists per query (a fixed number per split)
   uint32_t kblocks;
 };
 // Largest k the brute force accepts (candidates kept = k + 16 <= 128).
