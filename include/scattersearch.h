@@ -255,9 +255,14 @@ int ss_search_scatter_batch_device(ss_index *h, const float *queries, uint32_t n
  * but never changes results);
  * blocks_per_sm_cap: limit on resident CTAs per SM (0 = occupancy limit). */
 int ss_set_tuning(ss_index *h, int warps_per_block, int hash_cap, int blocks_per_sm_cap);
+/* Launches of at most 32 queries (single queries, small serving batches)
+ * ignore this tuning and the stage layout below: all their query teams fit
+ * on the GPU, so they take a latency layout (one 32-row stage per team, a
+ * visited table of about 20 x L slots, the CTA size that keeps the most
+ * teams resident).  Results are the same either way. */
 
 /* Row stages of the batched kernel.  stage_rows: base rows one stage holds
- * (1-16, 0 = 16); a hop with more fresh candidates than that copies and
+ * (1-32, 0 = 16); a hop with more fresh candidates than that copies and
  * evaluates them in several passes, and a smaller stage leaves room for more
  * query teams per SM.  stages_per_block: row stages shared by the query
  * teams of one CTA (0 = each team has its own; n > 0 = a pool of n stages

@@ -254,16 +254,17 @@ int stages_for(const ss_index *h, int wpb) {
 // Query teams per CTA: the tuned value when set, else the candidate (1, 2,
 // 4, 8) that keeps the most teams resident per SM (ties: larger CTAs).  The
 // plan's stage layout is set to match.
-int choose_wpb(ss_index *h, ssb::SmemPlan &p) {
+int choose_wpb(ss_index *h, ssb::SmemPlan &p, bool tuned = true) {
+  auto stages = [&](int w) { return tuned ? stages_for(h, w) : 0; };
   auto fits = [&](int w) {
     ssb::SmemPlan q = p;
-    ssb::share_stages(q, stages_for(h, w));
+    ssb::share_stages(q, stages(w));
     return ssb::warp_search_smem_bytes(q, w) <= 227 * 1024;
   };
-  if (h->warps_per_block > 0) {
+  if (tuned && h->warps_per_block > 0) {
     int wpb = h->warps_per_block;
     while (wpb > 1 && !fits(wpb)) wpb >>= 1;
-    ssb::share_stages(p, stages_for(h, wpb));
+    ssb::share_stages(p, stages(wpb));
     return wpb;
   }
   int best = 1, best_teams = -1;
@@ -275,8 +276,27 @@ int choose_wpb(ss_index *h, ssb::SmemPlan &p) {
       best = w;
     }
   }
-  ssb::share_stages(p, stages_for(h, best));
+  ssb::share_stages(p, stages(best));
   return best;
+}
+
+// Launches of at most kSmallLaunch queries use a latency layout whatever the
+// tuning (which is chosen for large batches, where shared memory per team
+// sets how many queries run at once): all their teams fit on the GPU anyway,
+// so each gets a 32-row stage (every fresh row of a hop arrives in one copy
+// round trip) and a visited table large enough to forget almost nothing
+// (fewer repeated evaluations), a stage of its own, and the CTA size that
+// keeps the most teams resident.
+constexpr uint32_t kSmallLaunch = 32;
+bool small_launch(uint32_t nq) { return nq <= kSmallLaunch; }
+int stage_rows_for(const ss_index *h, uint32_t nq) {
+  return small_launch(nq) ? 32 : h->stage_rows;
+}
+int hash_cap_for(const ss_index *h, uint32_t nq, int L_max) {
+  if (!small_launch(nq)) return h->hash_cap_override;
+  uint32_t slots = 1024;
+  while (slots < 16384u && slots < (uint32_t)L_max * 20u) slots <<= 1;
+  return (int)slots;
 }
 
 // Core batched launch into caller-provided device buffers on `stream`.
@@ -285,8 +305,8 @@ int launch_batch(ss_index *h, SearchCtx *c, const float *d_q, uint32_t nq, const
                  uint32_t *d_ids, float *d_dists, uint32_t *d_ndc, uint32_t *d_hops,
                  cudaStream_t stream, bool persistent) {
   ssb::GraphView g = h->view();
-  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, h->hash_cap_override, h->stage_rows);
-  const int wpb = choose_wpb(h, plan);
+  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, hash_cap_for(h, nq, L_max), stage_rows_for(h, nq));
+  const int wpb = choose_wpb(h, plan, !small_launch(nq));
   if (ssb::warp_search_smem_bytes(plan, wpb) > 227 * 1024)
     return set_err(h, SS_ERR_UNSUPPORTED, "L=%d needs %u bytes of shared memory per query",
                    L_max, plan.words_per_team * 4);
@@ -458,8 +478,8 @@ int server_launch(ss_index *h, const float *d_q, uint32_t nq, const int32_t *d_K
                   const int32_t *d_L, const int64_t *d_off, int L_max, uint32_t *d_ids,
                   float *d_dists, int32_t *d_status, uint32_t *d_counter, cudaStream_t stream) {
   ssb::GraphView g = h->view();
-  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, h->hash_cap_override, h->stage_rows);
-  const int wpb = choose_wpb(h, plan);
+  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, hash_cap_for(h, nq, L_max), stage_rows_for(h, nq));
+  const int wpb = choose_wpb(h, plan, !small_launch(nq));
   if (ssb::warp_search_smem_bytes(plan, wpb) > 227 * 1024)
     return set_err(h, SS_ERR_UNSUPPORTED, "L=%d needs %u bytes of shared memory per query",
                    L_max, plan.words_per_team * 4);
@@ -807,8 +827,8 @@ int ss_plan_create_uneven(ss_index *h, const float *queries, uint32_t nq, const 
   // Plan the launch outside the capture (occupancy queries and kernel
   // attributes are not stream work).
   ssb::GraphView g = h->view();
-  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, h->hash_cap_override, h->stage_rows);
-  const int wpb = choose_wpb(h, plan);
+  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, hash_cap_for(h, nq, L_max), stage_rows_for(h, nq));
+  const int wpb = choose_wpb(h, plan, !small_launch(nq));
   const int blocks = persistent_blocks(h, plan, wpb, nq);
   if (ssb::warp_search_smem_bytes(plan, wpb) > 227 * 1024 || blocks <= 0) {
     plan_free(p);
@@ -1087,8 +1107,8 @@ int ss_search_batch_noalloc(ss_index *h, const float *queries, uint32_t nq, int 
   DeviceGuard dg(h->device);
   const cudaStream_t st = static_cast<cudaStream_t>(stream);
   ssb::GraphView g = h->view();
-  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L, h->hash_cap_override, h->stage_rows);
-  const int wpb = choose_wpb(h, plan);
+  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L, hash_cap_for(h, nq, L), stage_rows_for(h, nq));
+  const int wpb = choose_wpb(h, plan, !small_launch(nq));
   if (ssb::warp_search_smem_bytes(plan, wpb) > 227 * 1024)
     return set_err(h, SS_ERR_UNSUPPORTED, "L=%d needs %u bytes of shared memory per query", L,
                    plan.words_per_team * 4);
@@ -1197,8 +1217,8 @@ int ss_set_tuning(ss_index *h, int warps_per_block, int hash_cap, int blocks_per
 
 int ss_set_stage_layout(ss_index *h, int stage_rows, int stages_per_block) {
   if (!h) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null index handle");
-  if (stage_rows < 0 || stage_rows > 16)
-    return set_err(h, SS_ERR_INVALID_ARGUMENT, "stage_rows must be in [0, 16]");
+  if (stage_rows < 0 || stage_rows > 32)
+    return set_err(h, SS_ERR_INVALID_ARGUMENT, "stage_rows must be in [0, 32]");
   if (stages_per_block < 0 || stages_per_block > 32)
     return set_err(h, SS_ERR_INVALID_ARGUMENT, "stages_per_block must be in [0, 32]");
   h->stage_rows = stage_rows;

@@ -38,6 +38,10 @@ constexpr uint32_t kExplored = 0x80000000u;
 // microseconds; the limit is far above that and only ends a wait that would
 // never finish).
 constexpr int kStageRows = 16;
+// Deepest whole-row stage: a hop has at most 32 fresh candidates (degree
+// <= 32 with one adjacency chunk), so a 32-row stage takes every row of a
+// hop in one copy round trip; its rows are computed in groups of 16.
+constexpr int kMaxStageRows = 32;
 constexpr uint32_t kStageWaitLimit = 1u << 24;
 
 // Number of a[0..n) with a[i] <= key (a ascending).
@@ -548,13 +552,24 @@ __device__ __forceinline__ bool eval_staged(const GraphView &g, const WarpSmem &
   const int h = lane & 1, c = lane >> 1;
   for (int p0 = 0; p0 < nc; p0 += srows) {
     const int m = min(srows, nc - p0);
-    const float *row = st.buf + (c < m ? c : 0) * p.stage_row_words;
-    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
     if (!split) {
       if (p0 > 0 || !first_issued) stage_issue(g, s, st, cid + p0, m, 2, p.stage_row_words, lane);
       if (!stage_wait(st)) return false;
-      staged_accumulate<NB, true>(g, s.q, row, h, 0, nb, a0, a1, a2, a3);
-    } else {
+      // one lane pair per row, 16 rows at a time
+      for (int g0 = 0; g0 < m; g0 += 16) {
+        const int mg = min(16, m - g0);
+        const float *rowg = st.buf + (g0 + (c < mg ? c : 0)) * p.stage_row_words;
+        float b0 = 0.f, b1 = 0.f, b2 = 0.f, b3 = 0.f;
+        staged_accumulate<NB, true>(g, s.q, rowg, h, 0, nb, b0, b1, b2, b3);
+        const float dg = pair_finish(g, h, b0, b1, b2, b3);
+        if (h == 0 && c < mg) ckey[p0 + g0 + c] = float_to_key(dg);
+      }
+      __syncwarp();
+      continue;
+    }
+    const float *row = st.buf + (c < m ? c : 0) * p.stage_row_words;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+    {
       if (p0 > 0 || !first_issued) stage_issue(g, s, st, cid + p0, m, 0, p.stage_row_words, lane);
       if (!stage_wait(st)) return false;
       staged_accumulate<NB, false>(g, s.q, row, h, 0, A, a0, a1, a2, a3);
@@ -1938,8 +1953,9 @@ SmemPlan plan_warp_smem(const GraphView &g, int L_max, int hash_cap_override, in
   // the cost of one L2 round trip per pass (measured slower than whole rows
   // at 200 dims: 546k against 640k queries/s at L = 400), and fewer rows
   // only beyond that.
-  const uint32_t rows = stage_rows > 0 ? (uint32_t)std::min(stage_rows, kStageRows) : kStageRows;
-  p.stage_split = rows * g.nb * 32u > 65536u ? 2 : 1;
+  uint32_t rows = stage_rows > 0 ? (uint32_t)std::min(stage_rows, kMaxStageRows) : kStageRows;
+  p.stage_split = kStageRows * g.nb * 32u > 65536u ? 2 : 1;
+  if (p.stage_split > 1) rows = std::min(rows, (uint32_t)kStageRows);  // split rows: 16 at most
   p.stage_row_words = (p.stage_split > 1 ? split_first(g.nb) : g.nb) * 8;
   p.stage_rows = rows;
   while (p.stage_rows > 1 && p.stage_rows * p.stage_row_words * 4u > 65536u) p.stage_rows >>= 1;

@@ -380,3 +380,29 @@ def test_graph_captured_uneven_plan(oracle_lib):
         assert _same_bits(d.cpu().numpy(), o_d)
     plan.close()
     idx.close()
+
+
+@pytest.mark.parametrize("name", ["search_l2_d200", "search_ip_d96"])
+def test_small_launches_and_deep_stages_keep_results(oracle_lib, name):
+    """Launches of at most 32 queries take the latency layout (32-row stages,
+    a larger visited table); a tuned 32-row stage serves large batches.
+    Every one returns the ids and distance bits of the large batch."""
+    fx = load_fixture(name)
+    idx = _index(fx["base"], fx["adj"], fx["ep"], int(fx["metric"]))
+    Q = fx["queries"]
+    K, L = 10, 100
+    ids, d = idx.search_batch(Q, K, L)
+    o_ids, o_d, _, _ = oracle_lib.search(fx["base"], fx["adj"], int(fx["ep"]),
+                                         int(fx["metric"]), Q, K, L)
+    assert np.array_equal(ids, o_ids) and _same_bits(d, o_d)
+    for lo, hi in ((0, 1), (3, 10), (10, 42)):
+        s_ids, s_d = idx.search_batch(Q[lo:hi], K, L)
+        assert np.array_equal(s_ids, ids[lo:hi]) and _same_bits(s_d, d[lo:hi]), (lo, hi)
+    one, one_d = idx.search(Q[5], K, L)
+    assert np.array_equal(one, ids[5]) and _same_bits(one_d, d[5])
+    for wpb, stages, rows in ((2, 0, 32), (4, 2, 24), (1, 0, 17)):
+        idx.set_tuning(warps_per_block=wpb, shared_stages=stages, stage_rows=rows)
+        t_ids, t_d = idx.search_batch(Q, K, L)
+        assert np.array_equal(t_ids, ids) and _same_bits(t_d, d), (wpb, stages, rows)
+    idx.set_tuning()
+    idx.close()
