@@ -537,7 +537,7 @@ __device__ __forceinline__ float pair_finish(const GraphView &g, int h, float a0
 // hits) into the same buffer.  When `first_issued`, the first load (part 0,
 // or the whole rows) was already started with stage_issue.  Returns false
 // when a stage wait timed out.
-template <int NB>
+template <int NB, bool DEEP>
 __device__ __forceinline__ bool eval_staged(const GraphView &g, const WarpSmem &s, RowStage &st,
                                             const StagePool &sp, const SmemPlan &p,
                                             const uint32_t *cid, uint32_t *ckey, int nc,
@@ -552,24 +552,30 @@ __device__ __forceinline__ bool eval_staged(const GraphView &g, const WarpSmem &
   const int h = lane & 1, c = lane >> 1;
   for (int p0 = 0; p0 < nc; p0 += srows) {
     const int m = min(srows, nc - p0);
-    if (!split) {
-      if (p0 > 0 || !first_issued) stage_issue(g, s, st, cid + p0, m, 2, p.stage_row_words, lane);
-      if (!stage_wait(st)) return false;
-      // one lane pair per row, 16 rows at a time
-      for (int g0 = 0; g0 < m; g0 += 16) {
-        const int mg = min(16, m - g0);
-        const float *rowg = st.buf + (g0 + (c < mg ? c : 0)) * p.stage_row_words;
-        float b0 = 0.f, b1 = 0.f, b2 = 0.f, b3 = 0.f;
-        staged_accumulate<NB, true>(g, s.q, rowg, h, 0, nb, b0, b1, b2, b3);
-        const float dg = pair_finish(g, h, b0, b1, b2, b3);
-        if (h == 0 && c < mg) ckey[p0 + g0 + c] = float_to_key(dg);
+    if constexpr (DEEP) {  // stages deeper than 16 rows: one wait, 16-row groups
+      if (!split) {
+        if (p0 > 0 || !first_issued)
+          stage_issue(g, s, st, cid + p0, m, 2, p.stage_row_words, lane);
+        if (!stage_wait(st)) return false;
+        for (int g0 = 0; g0 < m; g0 += 16) {
+          const int mg = min(16, m - g0);
+          const float *rowg = st.buf + (g0 + (c < mg ? c : 0)) * p.stage_row_words;
+          float b0 = 0.f, b1 = 0.f, b2 = 0.f, b3 = 0.f;
+          staged_accumulate<NB, true>(g, s.q, rowg, h, 0, nb, b0, b1, b2, b3);
+          const float dg = pair_finish(g, h, b0, b1, b2, b3);
+          if (h == 0 && c < mg) ckey[p0 + g0 + c] = float_to_key(dg);
+        }
+        __syncwarp();
+        continue;
       }
-      __syncwarp();
-      continue;
     }
     const float *row = st.buf + (c < m ? c : 0) * p.stage_row_words;
     float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-    {
+    if (!split) {
+      if (p0 > 0 || !first_issued) stage_issue(g, s, st, cid + p0, m, 2, p.stage_row_words, lane);
+      if (!stage_wait(st)) return false;
+      staged_accumulate<NB, true>(g, s.q, row, h, 0, nb, a0, a1, a2, a3);
+    } else {
       if (p0 > 0 || !first_issued) stage_issue(g, s, st, cid + p0, m, 0, p.stage_row_words, lane);
       if (!stage_wait(st)) return false;
       staged_accumulate<NB, false>(g, s.q, row, h, 0, A, a0, a1, a2, a3);
@@ -748,7 +754,7 @@ __device__ __forceinline__ void merge_accepted(const WarpSmem &s, int &size, int
 // After step 4 the next expansion is known (u, unless the best accepted
 // candidate lands before it), so its adjacency row loads during step 5, and
 // u's row is sent to L2 at the start of the hop.
-template <int NB, int RCH>
+template <int NB, int RCH, bool DEEP>
 __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qsrc, int K, int L,
                                 uint32_t *out_ids, float *out_dists, uint32_t *out_ndc,
                                 uint32_t *out_hops, int32_t *out_status, const WarpSmem &s,
@@ -792,7 +798,7 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
       size += __popc(__ballot_sync(kFull, valid));
     }
     __syncwarp();
-    if (!eval_staged<NB>(g, s, st, sp, p, s.cid, s.ckey, size, false, lane)) {
+    if (!eval_staged<NB, DEEP>(g, s, st, sp, p, s.cid, s.ckey, size, false, lane)) {
       status = kStatusStageTimeout;
       size = 0;
     }
@@ -899,7 +905,7 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
     __syncwarp();
 
     // 3. distances of the staged rows
-    if (!eval_staged<NB>(g, s, st, sp, p, s.cid, s.ckey, nc, issued, lane)) {
+    if (!eval_staged<NB, DEEP>(g, s, st, sp, p, s.cid, s.ckey, nc, issued, lane)) {
       status = kStatusStageTimeout;
       break;
     }
@@ -959,7 +965,7 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
 }
 
 // At most 128 registers a thread (two 256-thread CTAs' worth per SM).
-template <int NB, int RCH>
+template <int NB, int RCH, bool DEEP>
 __global__ void __launch_bounds__(256, 2) warp_search_kernel(GraphView g, BatchArgs a, SmemPlan p) {
   extern __shared__ __align__(128) uint32_t smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1008,7 +1014,7 @@ __global__ void __launch_bounds__(256, 2) warp_search_kernel(GraphView g, BatchA
     if (K < 1 || K > L || L > (int)p.pool_cap) {
       if (lane == 0 && a.status) a.status[q] = kStatusBadArgs;
     } else {
-      warp_search_one<NB, RCH>(g, a.queries + (size_t)q * a.qstride, K, L, a.ids + off,
+      warp_search_one<NB, RCH, DEEP>(g, a.queries + (size_t)q * a.qstride, K, L, a.ids + off,
                                a.dists ? a.dists + off : nullptr, a.ndc ? a.ndc + q : nullptr,
                                a.hops ? a.hops + q : nullptr, a.status ? a.status + q : nullptr, s,
                                p, st, sp, a.max_hops, lane);
@@ -1858,14 +1864,14 @@ __global__ void __launch_bounds__(512) scatter_search_kernel(GraphView g, BatchA
 using WarpFn = void (*)(GraphView, BatchArgs, SmemPlan);
 using IntraFn = void (*)(GraphView, BatchArgs, SmemPlan, int);
 
-template <int RCH>
+template <int RCH, bool DEEP>
 WarpFn warp_fn_for_nb(uint32_t nb) {
   switch (nb) {
-    case 8: return warp_search_kernel<8, RCH>;
-    case 12: return warp_search_kernel<12, RCH>;
-    case 16: return warp_search_kernel<16, RCH>;
-    case 25: return warp_search_kernel<25, RCH>;
-    default: return warp_search_kernel<0, RCH>;
+    case 8: return warp_search_kernel<8, RCH, DEEP>;
+    case 12: return warp_search_kernel<12, RCH, DEEP>;
+    case 16: return warp_search_kernel<16, RCH, DEEP>;
+    case 25: return warp_search_kernel<25, RCH, DEEP>;
+    default: return warp_search_kernel<0, RCH, DEEP>;
   }
 }
 template <int RCH>
@@ -1898,11 +1904,14 @@ ScatterFn scatter_fn(const GraphView &g, uint32_t pool_cap) {
   return scatter_fn_for_pool<4>(pool_cap);
 }
 
-WarpFn warp_fn(const GraphView &g) {
+// The DEEP instantiations (stages of more than 16 rows) are separate kernels,
+// so the code of the common 16-row kernel is unchanged by them.
+WarpFn warp_fn(const GraphView &g, const SmemPlan &p) {
   const uint32_t rch = (g.rstride + 31) / 32;
-  if (rch <= 1) return warp_fn_for_nb<1>(g.nb);
-  if (rch <= 2) return warp_fn_for_nb<2>(g.nb);
-  return warp_fn_for_nb<4>(g.nb);
+  const bool deep = p.stage_rows > (uint32_t)kStageRows;
+  if (rch <= 1) return deep ? warp_fn_for_nb<1, true>(g.nb) : warp_fn_for_nb<1, false>(g.nb);
+  if (rch <= 2) return deep ? warp_fn_for_nb<2, true>(g.nb) : warp_fn_for_nb<2, false>(g.nb);
+  return deep ? warp_fn_for_nb<4, true>(g.nb) : warp_fn_for_nb<4, false>(g.nb);
 }
 IntraFn intra_fn(const GraphView &g) {
   const uint32_t rch = (g.rstride + 31) / 32;
@@ -2059,7 +2068,7 @@ cudaError_t launch_scatter_search(const GraphView &g, const BatchArgs &a, const 
 }
 
 int warp_search_occupancy(const GraphView &g, const SmemPlan &p, int warps_per_block) {
-  WarpFn fn = warp_fn(g);
+  WarpFn fn = warp_fn(g, p);
   const size_t smem = warp_search_smem_bytes(p, warps_per_block);
   if (allow_max_smem((const void *)fn) != cudaSuccess) return 0;
   int blocks = 0;
@@ -2071,7 +2080,7 @@ int warp_search_occupancy(const GraphView &g, const SmemPlan &p, int warps_per_b
 
 cudaError_t launch_warp_search(const GraphView &g, const BatchArgs &a, const SmemPlan &p,
                                int warps_per_block, int blocks, cudaStream_t stream) {
-  WarpFn fn = warp_fn(g);
+  WarpFn fn = warp_fn(g, p);
   const size_t smem = warp_search_smem_bytes(p, warps_per_block);
   cudaError_t e = allow_max_smem((const void *)fn);
   if (e != cudaSuccess) return e;
