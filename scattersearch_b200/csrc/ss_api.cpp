@@ -287,13 +287,15 @@ int choose_wpb(ss_index *h, ssb::SmemPlan &p, bool tuned = true) {
 // round trip) and a visited table large enough to forget almost nothing
 // (fewer repeated evaluations), a stage of its own, and the CTA size that
 // keeps the most teams resident.
+// The serving loop runs a few launch slots at once; batches of up to
+// kServerSmallLaunch requests on each still fit on the GPU together with the
+// latency layout (four slots of 128 take 512 teams; about 590 fit at L = 400).
 constexpr uint32_t kSmallLaunch = 32;
-bool small_launch(uint32_t nq) { return nq <= kSmallLaunch; }
-int stage_rows_for(const ss_index *h, uint32_t nq) {
-  return small_launch(nq) ? 32 : h->stage_rows;
-}
-int hash_cap_for(const ss_index *h, uint32_t nq, int L_max) {
-  if (!small_launch(nq)) return h->hash_cap_override;
+constexpr uint32_t kServerSmallLaunch = 128;
+bool small_launch(uint32_t nq, uint32_t limit = kSmallLaunch) { return nq <= limit; }
+int stage_rows_for(const ss_index *h, bool small) { return small ? 32 : h->stage_rows; }
+int hash_cap_for(const ss_index *h, bool small, int L_max) {
+  if (!small) return h->hash_cap_override;
   uint32_t slots = 1024;
   while (slots < 16384u && slots < (uint32_t)L_max * 20u) slots <<= 1;
   return (int)slots;
@@ -305,7 +307,8 @@ int launch_batch(ss_index *h, SearchCtx *c, const float *d_q, uint32_t nq, const
                  uint32_t *d_ids, float *d_dists, uint32_t *d_ndc, uint32_t *d_hops,
                  cudaStream_t stream, bool persistent) {
   ssb::GraphView g = h->view();
-  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, hash_cap_for(h, nq, L_max), stage_rows_for(h, nq));
+  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, hash_cap_for(h, small_launch(nq), L_max),
+                                              stage_rows_for(h, small_launch(nq)));
   const int wpb = choose_wpb(h, plan, !small_launch(nq));
   if (ssb::warp_search_smem_bytes(plan, wpb) > 227 * 1024)
     return set_err(h, SS_ERR_UNSUPPORTED, "L=%d needs %u bytes of shared memory per query",
@@ -478,8 +481,10 @@ int server_launch(ss_index *h, const float *d_q, uint32_t nq, const int32_t *d_K
                   const int32_t *d_L, const int64_t *d_off, int L_max, uint32_t *d_ids,
                   float *d_dists, int32_t *d_status, uint32_t *d_counter, cudaStream_t stream) {
   ssb::GraphView g = h->view();
-  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, hash_cap_for(h, nq, L_max), stage_rows_for(h, nq));
-  const int wpb = choose_wpb(h, plan, !small_launch(nq));
+  const bool small = small_launch(nq, kServerSmallLaunch);
+  ssb::SmemPlan plan =
+      ssb::plan_warp_smem(g, L_max, hash_cap_for(h, small, L_max), stage_rows_for(h, small));
+  const int wpb = choose_wpb(h, plan, !small);
   if (ssb::warp_search_smem_bytes(plan, wpb) > 227 * 1024)
     return set_err(h, SS_ERR_UNSUPPORTED, "L=%d needs %u bytes of shared memory per query",
                    L_max, plan.words_per_team * 4);
@@ -827,7 +832,8 @@ int ss_plan_create_uneven(ss_index *h, const float *queries, uint32_t nq, const 
   // Plan the launch outside the capture (occupancy queries and kernel
   // attributes are not stream work).
   ssb::GraphView g = h->view();
-  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, hash_cap_for(h, nq, L_max), stage_rows_for(h, nq));
+  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, hash_cap_for(h, small_launch(nq), L_max),
+                                              stage_rows_for(h, small_launch(nq)));
   const int wpb = choose_wpb(h, plan, !small_launch(nq));
   const int blocks = persistent_blocks(h, plan, wpb, nq);
   if (ssb::warp_search_smem_bytes(plan, wpb) > 227 * 1024 || blocks <= 0) {
@@ -1107,7 +1113,8 @@ int ss_search_batch_noalloc(ss_index *h, const float *queries, uint32_t nq, int 
   DeviceGuard dg(h->device);
   const cudaStream_t st = static_cast<cudaStream_t>(stream);
   ssb::GraphView g = h->view();
-  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L, hash_cap_for(h, nq, L), stage_rows_for(h, nq));
+  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L, hash_cap_for(h, small_launch(nq), L),
+                                              stage_rows_for(h, small_launch(nq)));
   const int wpb = choose_wpb(h, plan, !small_launch(nq));
   if (ssb::warp_search_smem_bytes(plan, wpb) > 227 * 1024)
     return set_err(h, SS_ERR_UNSUPPORTED, "L=%d needs %u bytes of shared memory per query", L,
