@@ -280,6 +280,26 @@ int choose_wpb(ss_index *h, ssb::SmemPlan &p, bool tuned = true) {
   return best;
 }
 
+int small_hash_cap(int L_max);
+
+// Plans a warp-kernel launch of nq queries: the latency layout when nq is at
+// most small_limit and that layout fits in shared memory, else the tuned (or
+// automatic) layout.  Returns the plan; *wpb receives the teams per CTA.
+ssb::SmemPlan plan_launch(ss_index *h, const ssb::GraphView &g, int L_max, uint32_t nq,
+                          uint32_t small_limit, int *wpb) {
+  if (nq <= small_limit) {
+    ssb::SmemPlan p = ssb::plan_warp_smem(g, L_max, small_hash_cap(L_max), 32);
+    const int w = choose_wpb(h, p, false);
+    if (ssb::warp_search_smem_bytes(p, w) <= 227 * 1024) {
+      *wpb = w;
+      return p;
+    }
+  }
+  ssb::SmemPlan p = ssb::plan_warp_smem(g, L_max, h->hash_cap_override, h->stage_rows);
+  *wpb = choose_wpb(h, p, true);
+  return p;
+}
+
 // Launches of at most kSmallLaunch queries use a latency layout whatever the
 // tuning (which is chosen for large batches, where shared memory per team
 // sets how many queries run at once): all their teams fit on the GPU anyway,
@@ -292,10 +312,7 @@ int choose_wpb(ss_index *h, ssb::SmemPlan &p, bool tuned = true) {
 // latency layout (four slots of 128 take 512 teams; about 590 fit at L = 400).
 constexpr uint32_t kSmallLaunch = 32;
 constexpr uint32_t kServerSmallLaunch = 128;
-bool small_launch(uint32_t nq, uint32_t limit = kSmallLaunch) { return nq <= limit; }
-int stage_rows_for(const ss_index *h, bool small) { return small ? 32 : h->stage_rows; }
-int hash_cap_for(const ss_index *h, bool small, int L_max) {
-  if (!small) return h->hash_cap_override;
+int small_hash_cap(int L_max) {
   uint32_t slots = 1024;
   while (slots < 16384u && slots < (uint32_t)L_max * 20u) slots <<= 1;
   return (int)slots;
@@ -307,9 +324,8 @@ int launch_batch(ss_index *h, SearchCtx *c, const float *d_q, uint32_t nq, const
                  uint32_t *d_ids, float *d_dists, uint32_t *d_ndc, uint32_t *d_hops,
                  cudaStream_t stream, bool persistent) {
   ssb::GraphView g = h->view();
-  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, hash_cap_for(h, small_launch(nq), L_max),
-                                              stage_rows_for(h, small_launch(nq)));
-  const int wpb = choose_wpb(h, plan, !small_launch(nq));
+  int wpb = 1;
+  ssb::SmemPlan plan = plan_launch(h, g, L_max, nq, kSmallLaunch, &wpb);
   if (ssb::warp_search_smem_bytes(plan, wpb) > 227 * 1024)
     return set_err(h, SS_ERR_UNSUPPORTED, "L=%d needs %u bytes of shared memory per query",
                    L_max, plan.words_per_team * 4);
@@ -481,10 +497,8 @@ int server_launch(ss_index *h, const float *d_q, uint32_t nq, const int32_t *d_K
                   const int32_t *d_L, const int64_t *d_off, int L_max, uint32_t *d_ids,
                   float *d_dists, int32_t *d_status, uint32_t *d_counter, cudaStream_t stream) {
   ssb::GraphView g = h->view();
-  const bool small = small_launch(nq, kServerSmallLaunch);
-  ssb::SmemPlan plan =
-      ssb::plan_warp_smem(g, L_max, hash_cap_for(h, small, L_max), stage_rows_for(h, small));
-  const int wpb = choose_wpb(h, plan, !small);
+  int wpb = 1;
+  ssb::SmemPlan plan = plan_launch(h, g, L_max, nq, kServerSmallLaunch, &wpb);
   if (ssb::warp_search_smem_bytes(plan, wpb) > 227 * 1024)
     return set_err(h, SS_ERR_UNSUPPORTED, "L=%d needs %u bytes of shared memory per query",
                    L_max, plan.words_per_team * 4);
@@ -832,9 +846,8 @@ int ss_plan_create_uneven(ss_index *h, const float *queries, uint32_t nq, const 
   // Plan the launch outside the capture (occupancy queries and kernel
   // attributes are not stream work).
   ssb::GraphView g = h->view();
-  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L_max, hash_cap_for(h, small_launch(nq), L_max),
-                                              stage_rows_for(h, small_launch(nq)));
-  const int wpb = choose_wpb(h, plan, !small_launch(nq));
+  int wpb = 1;
+  ssb::SmemPlan plan = plan_launch(h, g, L_max, nq, kSmallLaunch, &wpb);
   const int blocks = persistent_blocks(h, plan, wpb, nq);
   if (ssb::warp_search_smem_bytes(plan, wpb) > 227 * 1024 || blocks <= 0) {
     plan_free(p);
@@ -1113,9 +1126,8 @@ int ss_search_batch_noalloc(ss_index *h, const float *queries, uint32_t nq, int 
   DeviceGuard dg(h->device);
   const cudaStream_t st = static_cast<cudaStream_t>(stream);
   ssb::GraphView g = h->view();
-  ssb::SmemPlan plan = ssb::plan_warp_smem(g, L, hash_cap_for(h, small_launch(nq), L),
-                                              stage_rows_for(h, small_launch(nq)));
-  const int wpb = choose_wpb(h, plan, !small_launch(nq));
+  int wpb = 1;
+  ssb::SmemPlan plan = plan_launch(h, g, L, nq, kSmallLaunch, &wpb);
   if (ssb::warp_search_smem_bytes(plan, wpb) > 227 * 1024)
     return set_err(h, SS_ERR_UNSUPPORTED, "L=%d needs %u bytes of shared memory per query", L,
                    plan.words_per_team * 4);
