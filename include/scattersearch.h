@@ -255,12 +255,13 @@ int ss_search_scatter_batch_device(ss_index *h, const float *queries, uint32_t n
  * but never changes results);
  * blocks_per_sm_cap: limit on resident CTAs per SM (0 = occupancy limit). */
 int ss_set_tuning(ss_index *h, int warps_per_block, int hash_cap, int blocks_per_sm_cap);
-/* Launches of at most 32 queries (single queries, small batches; for the
- * serving loop, batches of at most 128 requests) ignore this tuning and the
- * stage layout below: all their query teams fit on the GPU, so they take a
+/* Launches whose queries can all be resident on the GPU at once in a
  * latency layout (one 32-row stage per team, a visited table of about
- * 20 x L slots, the CTA size that keeps the most teams resident).  Results
- * are the same either way. */
+ * 20 x L slots, the CTA size that keeps the most teams resident) take that
+ * layout and ignore this tuning and the stage layout below: about 1000
+ * queries at dim 200 and L = 100, 590 at L = 400.  The serving loop's
+ * launches take it for batches of at most 128 requests.  Results are the
+ * same either way. */
 
 /* Row stages of the batched kernel.  stage_rows: base rows one stage holds
  * (1-32, 0 = 16); a hop with more fresh candidates than that copies and

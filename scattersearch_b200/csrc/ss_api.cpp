@@ -282,17 +282,28 @@ int choose_wpb(ss_index *h, ssb::SmemPlan &p, bool tuned = true) {
 
 int small_hash_cap(int L_max);
 
-// Plans a warp-kernel launch of nq queries: the latency layout when nq is at
-// most small_limit and that layout fits in shared memory, else the tuned (or
-// automatic) layout.  Returns the plan; *wpb receives the teams per CTA.
+// Plans a warp-kernel launch of nq queries.  The latency layout (one 32-row
+// stage and a large visited table per team, untuned CTA size) is taken when
+// it fits in shared memory and nq is at most `small_limit` -- or, with
+// small_limit 0, when every query of the launch can be resident at once in
+// it: all queries then run together in either layout, and this one finishes
+// each sooner.  Otherwise the tuned (or automatic) layout is used.  Returns
+// the plan; *wpb receives the teams per CTA.
 ssb::SmemPlan plan_launch(ss_index *h, const ssb::GraphView &g, int L_max, uint32_t nq,
                           uint32_t small_limit, int *wpb) {
-  if (nq <= small_limit) {
+  {
     ssb::SmemPlan p = ssb::plan_warp_smem(g, L_max, small_hash_cap(L_max), 32);
     const int w = choose_wpb(h, p, false);
     if (ssb::warp_search_smem_bytes(p, w) <= 227 * 1024) {
-      *wpb = w;
-      return p;
+      uint32_t limit = small_limit;
+      if (limit == 0) {
+        const int per_sm = ssb::warp_search_occupancy(g, p, w);
+        limit = (uint32_t)std::max(per_sm, 0) * (uint32_t)w * (uint32_t)h->sm_count;
+      }
+      if (nq <= limit) {
+        *wpb = w;
+        return p;
+      }
     }
   }
   ssb::SmemPlan p = ssb::plan_warp_smem(g, L_max, h->hash_cap_override, h->stage_rows);
@@ -300,17 +311,16 @@ ssb::SmemPlan plan_launch(ss_index *h, const ssb::GraphView &g, int L_max, uint3
   return p;
 }
 
-// Launches of at most kSmallLaunch queries use a latency layout whatever the
-// tuning (which is chosen for large batches, where shared memory per team
-// sets how many queries run at once): all their teams fit on the GPU anyway,
-// so each gets a 32-row stage (every fresh row of a hop arrives in one copy
-// round trip) and a visited table large enough to forget almost nothing
-// (fewer repeated evaluations), a stage of its own, and the CTA size that
-// keeps the most teams resident.
-// The serving loop runs a few launch slots at once; batches of up to
-// kServerSmallLaunch requests on each still fit on the GPU together with the
-// latency layout (four slots of 128 take 512 teams; about 590 fit at L = 400).
-constexpr uint32_t kSmallLaunch = 32;
+// Launches whose queries all fit on the GPU at once in the latency layout
+// (plan_launch with limit 0) take it whatever the tuning, which is chosen
+// for large batches where shared memory per team sets how many queries run
+// at once.  Each team then gets a 32-row stage (every fresh row of a hop
+// arrives in one copy round trip), a visited table large enough to forget
+// almost nothing (fewer repeated evaluations), and the CTA size that keeps
+// the most teams resident.  The serving loop runs a few launch slots at
+// once, so its launches use a fixed limit: four slots of 128 requests take
+// 512 teams, and about 590 fit at L = 400.
+constexpr uint32_t kSmallLaunch = 0;
 constexpr uint32_t kServerSmallLaunch = 128;
 int small_hash_cap(int L_max) {
   uint32_t slots = 1024;

@@ -24,6 +24,13 @@ def _index(base, adj, ep, metric):
     return idx
 
 
+def _tile(x, n=2700):
+    """Rows of x repeated to at least n: a batch too large to be resident at
+    once in the latency layout, so launches take the tuned layout."""
+    reps = -(-n // len(x))
+    return np.concatenate([x] * reps)
+
+
 def _same_bits(a, b):
     return np.array_equal(np.asarray(a, np.float32).view(np.uint32),
                           np.asarray(b, np.float32).view(np.uint32))
@@ -59,13 +66,17 @@ def test_batched_equals_plain(oracle_lib, name):
                                     fx["queries"], K, L)
         assert np.array_equal(ids, o_ids)
         assert _same_bits(d, o_d)
-        # launch layouts: teams per CTA, with a stage per team or a shared
-        # pool of fewer stages (a single shared stage included)
+        # launch layouts (on a batch large enough to take them): teams per
+        # CTA, with a stage per team or a shared pool of fewer stages (a
+        # single shared stage included), stage depths from 1 to 32 rows
+        big = _tile(fx["queries"])
+        reps = len(big) // len(fx["queries"])
         for wpb, stages, rows in ((1, 0, 0), (2, 0, 0), (8, 0, 0), (4, 1, 0), (8, 3, 0),
-                                  (8, 6, 0), (1, 0, 12), (2, 0, 5), (4, 2, 1)):
+                                  (8, 6, 0), (1, 0, 12), (2, 0, 5), (4, 2, 1), (2, 0, 32)):
             idx.set_tuning(warps_per_block=wpb, shared_stages=stages, stage_rows=rows)
-            ids2, d2 = idx.search_batch(fx["queries"], K, L)
-            assert np.array_equal(ids2, ids) and _same_bits(d2, d), (wpb, stages, rows)
+            ids2, d2 = idx.search_batch(big, K, L)
+            assert np.array_equal(ids2, np.tile(ids, (reps, 1))), (wpb, stages, rows)
+            assert _same_bits(d2, np.tile(d, (reps, 1))), (wpb, stages, rows)
         idx.set_tuning()
     idx.close()
 
@@ -149,13 +160,17 @@ def test_visited_spill_to_global_bitset(oracle_lib):
     idx = _index(X, adj, ep, 0)
     o_ids, o_d, ndc, _ = O.search(X, adj, ep, 0, Q, 50, 400)
     assert ndc.max() > 1024  # the smallest visited table (512 slots) must overflow
+    # a batch too large for the latency layout, so the 512-slot tables run
+    big = _tile(Q)
+    reps = len(big) // len(Q)
+    o_big_ids, o_big_d = np.tile(o_ids, (reps, 1)), np.tile(o_d, (reps, 1))
     idx.set_tuning(warps_per_block=4, hash_cap=512)
     for _ in range(2):  # second pass checks the bitsets were cleared
-        ids, d = idx.search_batch(Q, 50, 400)
-        assert np.array_equal(ids, o_ids) and _same_bits(d, o_d)
+        ids, d = idx.search_batch(big, 50, 400)
+        assert np.array_equal(ids, o_big_ids) and _same_bits(d, o_big_d)
     idx.set_tuning(warps_per_block=8, hash_cap=512, shared_stages=2)
-    ids, d = idx.search_batch(Q, 50, 400)
-    assert np.array_equal(ids, o_ids) and _same_bits(d, o_d)
+    ids, d = idx.search_batch(big, 50, 400)
+    assert np.array_equal(ids, o_big_ids) and _same_bits(d, o_big_d)
     idx.set_tuning(warps_per_block=4, hash_cap=512)
     for W in (1, 4):
         o_w, _, _, _ = O.search(X, adj, ep, 0, Q[:16], 50, 400, W=W)
@@ -384,9 +399,10 @@ def test_graph_captured_uneven_plan(oracle_lib):
 
 @pytest.mark.parametrize("name", ["search_l2_d200", "search_ip_d96"])
 def test_small_launches_and_deep_stages_keep_results(oracle_lib, name):
-    """Launches of at most 32 queries take the latency layout (32-row stages,
-    a larger visited table); a tuned 32-row stage serves large batches.
-    Every one returns the ids and distance bits of the large batch."""
+    """Launches whose queries all fit on the GPU at once take the latency
+    layout (32-row stages, a larger visited table); tuned layouts, 32-row
+    stages among them, serve batches too large for that.  Every one returns
+    the ids and distance bits of the oracle."""
     fx = load_fixture(name)
     idx = _index(fx["base"], fx["adj"], fx["ep"], int(fx["metric"]))
     Q = fx["queries"]
@@ -400,9 +416,12 @@ def test_small_launches_and_deep_stages_keep_results(oracle_lib, name):
         assert np.array_equal(s_ids, ids[lo:hi]) and _same_bits(s_d, d[lo:hi]), (lo, hi)
     one, one_d = idx.search(Q[5], K, L)
     assert np.array_equal(one, ids[5]) and _same_bits(one_d, d[5])
+    big = _tile(Q)
+    reps = len(big) // len(Q)
     for wpb, stages, rows in ((2, 0, 32), (4, 2, 24), (1, 0, 17)):
         idx.set_tuning(warps_per_block=wpb, shared_stages=stages, stage_rows=rows)
-        t_ids, t_d = idx.search_batch(Q, K, L)
-        assert np.array_equal(t_ids, ids) and _same_bits(t_d, d), (wpb, stages, rows)
+        t_ids, t_d = idx.search_batch(big, K, L)
+        assert np.array_equal(t_ids, np.tile(ids, (reps, 1))), (wpb, stages, rows)
+        assert _same_bits(t_d, np.tile(d, (reps, 1))), (wpb, stages, rows)
     idx.set_tuning()
     idx.close()
