@@ -9,14 +9,24 @@
 // right.  That makes the GPU results bit-identical to the reference built
 // without fast-math.
 //
-// Two kernels:
+// Three kernels:
 //   warp_search_kernel   one warp owns one query (pool, visited hash and
 //                        candidate buffers in shared memory); a CTA holds
 //                        several independent query teams; teams pull queries
 //                        from a device work counter until the batch is empty
-//                        (persistent) or take them by index (static).
+//                        (persistent) or take them by index (static).  Base
+//                        rows reach each team through a row stage filled by
+//                        bulk copies: a team's own stage, or one taken from a
+//                        pool the CTA's teams share.  Stages deeper than 16
+//                        rows (one copy round trip per hop) are a separate
+//                        instantiation (DEEP), used for launches small
+//                        enough to keep every query resident.
 //   intra_search_kernel  one CTA owns one query; each step expands the W best
 //                        unexplored entries at once, one per warp.
+//   scatter_search_kernel  ScatterSearch's own intra-query search: one CTA
+//                        per query, a pool per warp from its own entry point,
+//                        one shared visited set, optional election and early
+//                        termination.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
