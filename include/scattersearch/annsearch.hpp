@@ -138,10 +138,13 @@ class ANNSearch {
                  handle, "SearchBatchUneven");
   }
 
-  // Launch tuning of the batched kernel (ss_set_tuning; 0 = automatic).
-  void SetTuning(int warps_per_block = 0, int hash_cap = 0, int blocks_per_sm_cap = 0) {
+  // Launch tuning of the batched kernel (ss_set_tuning and
+  // ss_set_stage_layout; 0 = automatic).  Results never depend on it.
+  void SetTuning(int warps_per_block = 0, int hash_cap = 0, int blocks_per_sm_cap = 0,
+                 int shared_stages = 0, int stage_rows = 0) {
     die_on_error(ss_set_tuning(handle, warps_per_block, hash_cap, blocks_per_sm_cap), handle,
                  "SetTuning");
+    die_on_error(ss_set_stage_layout(handle, stage_rows, shared_stages), handle, "SetTuning");
   }
 
   std::vector<uint32_t> graph_table(unsigned rstride) const {
