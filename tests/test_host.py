@@ -248,3 +248,43 @@ def test_data_tools_split_and_convert(tmp_path):
     assert np.array_equal(sio.load_groundtruth(paths[2]), nbr[:, :10].astype(np.uint32))
     with pytest.raises(ValueError):
         sio.ann_benchmarks_to_fbin(train, test, nbr + 500, *paths)
+
+
+def test_bench_clock_samples_and_profiled_traffic(tmp_path, monkeypatch):
+    """The bench's clock record (median SM clock, throttle reasons, the
+    one-shot fallback when no sample landed in the window) and the DRAM
+    traffic it reads from the committed ncu summary."""
+    import bench
+
+    class Done:
+        def terminate(self):
+            pass
+
+        def wait(self, timeout=None):
+            return 0
+
+    rows = ["0, 1965, 1965, 700.1, 0x0, Not Active, Not Active, Not Active, Not Active",
+            "0, 1950, 1965, 980.0, 0x4, Not Active, Not Active, Not Active, Active",
+            "0, 1965, 1965, 990.5, 0x4, Not Active, Not Active, Not Active, Active"]
+    s = bench.ClockSampler(0)
+    s.path = str(tmp_path / "clk.csv")
+    s.proc = Done()
+    s.skip = 1  # a sample from before the warm-up is dropped
+    with open(s.path, "w") as f:
+        f.write("0, 900, 1965, 100.0, 0x0, Not Active, Active, Not Active, Not Active\n")
+        f.write("\n".join(rows) + "\n")
+    c = s.stop()
+    assert c["samples"] == 3 and c["sm_mhz"] == 1965.0 and c["sm_max_mhz"] == 1965.0
+    assert c["reasons"] == ["sw_power_cap"] and c["window"] == "warm-up and timed steps"
+    # nothing inside the steps: one read right after them
+    s2 = bench.ClockSampler(0)
+    s2.path = str(tmp_path / "clk2.csv")
+    s2.proc = Done()
+    open(s2.path, "w").close()
+    monkeypatch.setattr(bench.ClockSampler, "_one_shot", lambda self: rows[:1])
+    c2 = s2.stop()
+    assert c2["samples"] == 1 and c2["window"] == "right after the timed steps"
+    # the roofline's traffic comes from the committed summary of the same workload
+    traffic, src = bench.profiled_traffic("cfg3", 400, 10000)
+    assert src.endswith(".md") and 6e10 < traffic < 8e10
+    assert bench.profiled_traffic("cfg3", 200, 10000) == (None, None)
