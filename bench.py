@@ -2,7 +2,7 @@
 """Benchmark of the graph-search hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload cfg3|cfg2|cfg1] [--L auto|<int>] [--nq Q] [--scale S]
+                    [--workload cfg3|cfg2|cfg1|cfg4] [--L auto|<int>] [--nq Q] [--scale S]
 
 Workload (default): the 1.2M x 200 angular configuration -- seeded
 50-component Gaussian mixture, unit-normalised, inner product, K = 100, an
@@ -21,6 +21,11 @@ cores over a bounded sample.
 
 --impl reference times that reference CPU search alone as the reference arm
 (same workload; rank 0 only under torchrun).
+
+--workload cfg4: one batch of 100k queries with per-query K in {1, 10, 100}
+and L in [32, 512] over 5M x 96 unit vectors, searched by one persistent
+launch captured in a CUDA graph; its CPU baseline is the oracle's C
+restatement (the reference's drivers take one K and L per run).
 
 Multi-GPU (torchrun, one rank per GPU): every rank holds a replica of the
 index and searches its own 10k queries (weak scaling, no device collective);
