@@ -91,7 +91,13 @@ def parse_args(argv=None):
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-online", action="store_true",
-                    help="skip the serving and intra-query latency legs")
+                    help="skip the serving, intra-query and ScatterSearch latency legs")
+    ap.add_argument("--no-config1", action="store_true", help="skip the configuration-1 leg")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the id-parity record against the parity-built reference")
+    ap.add_argument("--layout", default=None,
+                    help="fixed launch layout 'teams_per_cta,table_slots,shared_stages,stage_rows' "
+                         "instead of the autotuner's (profiling)")
     args = ap.parse_args(argv)
     if args.nq is None:
         args.nq = 100_000 if args.workload == "cfg4" else 10_000
@@ -245,8 +251,10 @@ def workload_spec(name):
     return dict(cfg=1, Ls=[100, 200], K=10, desc="100kx200 L2, K=10")
 
 
-def build_workload(args, rank, world, device):
-    """Seeded data, NSG-style graph and exact ground truth (setup, untimed)."""
+def build_workload(args, rank, world, device, gt_kernel=True):
+    """Seeded data, NSG-style graph and exact ground truth (setup, untimed).
+    gt_kernel=False takes the ground truth from torch (float32 scan, float64
+    re-rank), so the process never loads the project's library."""
     import torch
     from scattersearch_b200 import datasets, graph
     spec = workload_spec(args.workload)
@@ -266,25 +274,29 @@ def build_workload(args, rank, world, device):
     if device != "cpu" and torch.cuda.is_available():
         torch.cuda.empty_cache()  # hand the graph build's scratch back to the driver
     ns = min(len(queries), spec.get("gt_sample", len(queries)))
-    gt, gt_info = ground_truth(X, Q[:ns], w.metric, device)
+    gt, gt_info = ground_truth(X, Q[:ns], w.metric, device, use_library=gt_kernel)
     log(f"ground truth: {gt_info}")
     return dict(spec=spec, w=w, X=X, queries=queries, Q=Q, adj=adj, ep=ep,
                 gt=gt, gt_info=gt_info, metric=w.metric, K=spec["K"])
 
 
-def ground_truth(X, Q, metric, device, k=10):
+def ground_truth(X, Q, metric, device, k=10, use_library=True):
     """Exact top-10 of every query: the library's tensor-core brute force
-    (timed with CUDA events), or torch when the library is not built."""
+    (timed with CUDA events), or torch (float32 candidate scan, float64
+    re-rank) when use_library is off or the library is not built."""
     import torch
     nq, dim = Q.shape
     n = X.shape[0]
     try:
+        if not use_library:
+            raise LookupError("torch ground truth requested")
         from scattersearch_b200 import ANNSearch
         idx = ANNSearch(dim, n, X, metric, base_on_device=True)
-    except Exception as e:  # library missing (e.g. a CPU-only run)
+    except Exception as e:  # torch requested, or the library missing (a CPU-only run)
         from scattersearch_b200 import graph
         gt, _ = graph.bruteforce(X, Q, k, metric)
-        return gt.cpu().numpy(), {"kernel": f"torch ({e.__class__.__name__})"}
+        return gt.cpu().numpy().astype(np.uint32), {
+            "kernel": "torch float32 scan + float64 re-rank (" + str(e) + ")"}
     ids = torch.empty((nq, k), dtype=torch.int32, device=device)
     st = torch.cuda.current_stream()
     idx.bruteforce_device(Q, nq, k, ids, stream=st.cuda_stream)  # warm-up (norms, attributes)
@@ -303,9 +315,11 @@ def ground_truth(X, Q, metric, device, k=10):
 
 
 def recall_at_10(ids, gt):
+    """Mean share of each row's first 10 ids found among its 10 true
+    neighbours (the reference drivers' recall@K, tests/search.cpp:90-104)."""
     ids = np.asarray(ids)[:, :10].astype(np.int64)
-    hit = [(np.isin(ids[i], gt[i])).sum() for i in range(len(ids))]
-    return float(np.mean(hit) / 10.0)
+    gt = np.asarray(gt)[:len(ids), :10].astype(np.int64)
+    return float((ids[:, :, None] == gt[:, None, :]).any(2).mean())
 
 
 # -------------------------------------------------------- reference arm
@@ -353,6 +367,17 @@ def run_reference_arm(args):
     return 0
 
 
+def library_mapped():
+    """Shared objects of this project mapped into this process (from
+    /proc/self/maps): the reference arm must map none of the product's."""
+    try:
+        with open("/proc/self/maps") as f:
+            paths = {ln.split()[-1] for ln in f if ln.rstrip().endswith(".so")}
+    except OSError:
+        return None
+    return sorted(os.path.relpath(p, ROOT) for p in paths if p.startswith(ROOT))
+
+
 def _reference_arm(args):
     d = Dist("gloo")
     if d.rank != 0:
@@ -368,67 +393,62 @@ def _reference_arm(args):
         d.close()
         return {"impl": "reference", "unavailable": "oracle/_ref/libssref_fast.so was not built"}
     device = torch.device("cuda", d.local_rank) if torch.cuda.is_available() else "cpu"
-    wl = build_workload(args, 0, 1, device)
-    L = choose_L_reference(args, wl)
+    # setup only: the index's graph is built with torch and the ground truth
+    # comes from torch, so nothing of the project's library is loaded here
+    wl = build_workload(args, 0, 1, device, gt_kernel=False)
     th = cpu_threads()
     ref = O.RefIndex(wl["w"].base, wl["metric"], wl["adj"], wl["ep"], fast=True)
     K, q = wl["K"], wl["queries"]
-    probe = min(len(q), max(8 * th, 32))
-    t0 = time.perf_counter()
-    ref.search(q[:probe], K, L, nthreads=th)
-    rate = probe / max(1e-6, time.perf_counter() - t0)
-    # a step is a bounded sample of the workload: about cpu_seconds/steps of
-    # host work, the whole batch repeated when it is shorter than that
-    per_step = int(min(len(q), max(probe, rate * args.cpu_seconds / max(1, args.steps))))
-    reps = max(1, int(round(rate * args.cpu_seconds / max(1, args.steps) / per_step)))
+    L, sweep = reference_L(args, wl, ref, th)
+    # a step searches the same queries as a step of the GPU arm: all of them
     for _ in range(args.warmup):
-        ref.search(q[:min(per_step, probe)], K, L, nthreads=th)
+        ref.search(q, K, L, nthreads=th)
     times = []
     ids = None
-    for s in range(args.steps):
+    for _ in range(args.steps):
         t0 = time.perf_counter()
-        for _ in range(reps):
-            ids = ref.search(q[:per_step], K, L, nthreads=th)
+        ids = ref.search(q, K, L, nthreads=th)
         times.append(time.perf_counter() - t0)
     ref.close()
     total = sum(times)
-    qps = per_step * reps * args.steps / total
-    rec = recall_at_10(ids, wl["gt"][:per_step])
-    sample = (f"first {per_step} of {len(q)} queries x{reps} per step, K={K}, L={L}, "
-              f"-Ofast build, OpenMP over queries, one visited bitset per thread")
+    qps = len(q) * args.steps / total
+    rec = recall_at_10(ids, wl["gt"][:len(ids)])
+    sample = (f"all {len(q)} queries per step, K={K}, L={L}, reference SearchArraySimulation "
+              f"built -Ofast, OpenMP over queries, one visited bitset per thread")
     out = {
         "impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000 * total / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": wl["w"].name + " (synthetic, seeded)",
-        "config": {"workload": wl["spec"]["desc"], "K": K, "L": L, "nq_per_step": per_step,
-                   "recall@10": rec, "graph": "NSG-style, R<=32, built on the device (setup)"},
+        "config": {"workload": wl["spec"]["desc"] + f", {len(q)} queries per step",
+                   "K": K, "L": L, "nq_per_step": len(q), "recall@10": rec, "L_sweep": sweep,
+                   "graph": f"NSG-style, R<={wl['w'].graph_R}, built with torch (setup)",
+                   "ground_truth": wl["gt_info"]},
         "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": th, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "project_libraries_mapped": library_mapped(),
     }
     d.close()
     return out
 
 
-def choose_L_reference(args, wl):
+def reference_L(args, wl, ref, th, target=0.95):
+    """Beam width of the reference arm: --L, else the smallest configured L
+    whose recall@10 with the reference's own search reaches the target."""
     if args.L != "auto":
-        return int(args.L)
-    # same rule as our arm: smallest configured L whose GPU-free recall check
-    # passes is not affordable on the host, so use the GPU search to pick it
-    # when the library is present, else the largest configured L.
-    try:
-        from scattersearch_b200 import ANNSearch
-        idx = ANNSearch(wl["X"].shape[1], wl["X"].shape[0], wl["X"], wl["metric"],
-                        base_on_device=True)
-        idx.SetGraph(wl["adj"], wl["ep"])
-        L = pick_L(idx, wl)[0]
-        idx.close()
-        return L
-    except Exception as e:  # library missing: fall back to the configured maximum
-        log(f"L selection without the GPU library ({e}); using the largest configured L")
-        return wl["spec"]["Ls"][-1]
+        return int(args.L), []
+    sweep = []
+    q, gt = wl["queries"], wl["gt"]
+    for L in wl["spec"]["Ls"]:
+        ids = ref.search(q[:len(gt)], wl["K"], L, nthreads=th)
+        r = recall_at_10(ids, gt)
+        sweep.append((L, r))
+        log(f"reference L={L} recall@10={r:.4f}")
+        if r >= target:
+            return L, sweep
+    return sweep[-1][0], sweep
 
 
 # -------------------------------------------------------------- our arm
@@ -444,34 +464,223 @@ def pick_L(idx, wl, target=0.95):
     return res[-1][0], res[-1][1], res
 
 
-def measure_online(idx, wl, L, rates=(100_000, 300_000, 550_000), seconds=0.15):
-    """Serving leg: Poisson arrivals replayed through the continuous-batching
-    server (ss_server_replay); latency is arrival to result on the host."""
+def measure_online(idx, wl, rates=(1_000, 10_000, 50_000, 100_000, 200_000),
+                   saturation=2_000_000, seconds=1.0, max_requests=200_000, seed=5005):
+    """Serving leg, configuration 5: Poisson arrivals replayed through the
+    continuous-batching server (ss_server_replay) at each offered rate, for
+    max(1 s, 2000 requests) of arrivals (at most max_requests), then one
+    saturating burst.  Every request draws K from {10, 100} and L uniformly
+    from [64, 400] (L >= K); batches hold 1-256 requests.  Latency runs from
+    the scheduled arrival to the result on the host; recall@10 is over the
+    requests with K >= 10 (all of them)."""
     from scattersearch_b200.serving import Server, poisson_arrivals
-    K = wl["K"]
-    Q = wl["queries"]
+    Q, gt = wl["queries"], wl["gt"]
+    nq = min(len(Q), len(gt))
+    rng = np.random.default_rng(seed)
     out = []
-    with Server(idx, max_batch=512, max_inflight=4, K_max=K, L_max=L) as srv:
-        warm = min(len(Q), 4096)
-        srv.replay(Q[:warm], np.full(warm, K, np.int32), np.full(warm, L, np.int32),
+    with Server(idx, max_batch=256, max_inflight=4, K_max=100, L_max=400) as srv:
+        warm = min(nq, 4096)
+        srv.replay(Q[:warm], np.full(warm, 100, np.int32), np.full(warm, 400, np.int32),
                    poisson_arrivals(warm, 100_000, seed=1))
         srv.stats(reset=True)
-        for rate in rates:
-            n = int(max(2000, rate * seconds))
-            q = Q[np.arange(n) % len(Q)]
+        for rate in tuple(rates) + (saturation,):
+            n = int(min(max_requests, max(2000, rate * seconds)))
+            sel = np.arange(n) % nq
+            Ks = rng.choice(np.array([10, 100], np.int32), n)
+            Ls = np.maximum(Ks, rng.integers(64, 401, n)).astype(np.int32)
             t0 = time.perf_counter()
-            _, _, _, lat = srv.replay(q, np.full(n, K, np.int32), np.full(n, L, np.int32),
-                                      poisson_arrivals(n, rate, seed=rate))
+            ids, _, off, lat = srv.replay(Q[sel], Ks, Ls, poisson_arrivals(n, rate, seed=rate))
             wall = time.perf_counter() - t0
             st = srv.stats(reset=True)
-            out.append({"offered_qps": rate, "requests": n, "sustained_qps": n / wall,
-                        "p50_ms": float(np.percentile(lat, 50)) / 1e3,
-                        "p99_ms": float(np.percentile(lat, 99)) / 1e3,
-                        "p999_ms": float(np.percentile(lat, 99.9)) / 1e3,
-                        "mean_batch": st["mean_batch"]})
-            log(f"online {rate}/s: p50 {out[-1]['p50_ms']:.2f} ms p99 {out[-1]['p99_ms']:.2f} ms")
-    return {"K": K, "L": L, "max_batch": 512, "slots": 4, "arrivals": "Poisson",
-            "latency": "arrival to result on the host", "rates": out}
+            first10 = ids[off[:, None] + np.arange(10)[None, :]]
+            row = {"offered_qps": rate if rate != saturation else None,
+                   "saturating_burst": rate == saturation, "requests": n,
+                   "sustained_qps": n / wall,
+                   "p50_ms": float(np.percentile(lat, 50)) / 1e3,
+                   "p99_ms": float(np.percentile(lat, 99)) / 1e3,
+                   "p999_ms": float(np.percentile(lat, 99.9)) / 1e3,
+                   "recall@10": recall_at_10(first10, gt[sel]),
+                   "mean_batch": st["mean_batch"]}
+            out.append(row)
+            log(f"online {rate}/s: sustained {row['sustained_qps']:.0f}/s p50 {row['p50_ms']:.2f} "
+                f"p99 {row['p99_ms']:.2f} p999 {row['p999_ms']:.2f} ms recall {row['recall@10']:.4f}")
+    return {"K": "10 or 100 per request", "L": "uniform in [64, 400] per request",
+            "max_batch": 256, "slots": 4, "arrivals": "Poisson",
+            "window": f"max({seconds:g} s, 2000 requests) per rate, at most {max_requests}",
+            "latency": "scheduled arrival to result on the host", "rates": out}
+
+
+def parity_record(wl, ids_np, L):
+    """The reference's own SearchArraySimulation, built with parity flags
+    (oracle/_ref/libssref.so: -O2, no FMA contraction), on every bench
+    query: the share of id lists equal to the GPU's, overall and over the
+    queries whose initial pool has no exact distance tie between distinct ids
+    (std::sort leaves those in an implementation-defined order), and recall@10
+    of both against the same ground truth."""
+    from oracle import oracle as O
+    if not O.have_reference():
+        return None
+    th = cpu_threads()
+    w, K = wl["w"], wl["K"]
+    q = wl["queries"]
+    ref = O.RefIndex(w.base, wl["metric"], wl["adj"], wl["ep"])
+    t0 = time.perf_counter()
+    with stdout_to_stderr():
+        r_ids = ref.search(q, K, L, nthreads=th)
+    dt = time.perf_counter() - t0
+    ref.close()
+    tie = O.init_ties(w.base, wl["adj"], wl["ep"], q, L, wl["metric"])
+    same = (r_ids == ids_np).all(1)
+    ng = len(wl["gt"])
+    return {"reference": "SearchArraySimulation (src/annsearch.cpp:182-259), parity build "
+                         "oracle/_ref/libssref.so", "queries": int(len(q)), "K": K, "L": L,
+            "init_tie_queries": int(tie.sum()),
+            "ids_equal_fraction": float(same.mean()),
+            "ids_equal_fraction_excluding_init_ties": float(same[~tie].mean()) if (~tie).any()
+            else None,
+            "recall@10_gpu": recall_at_10(ids_np[:ng], wl["gt"]),
+            "recall@10_reference": recall_at_10(r_ids[:ng], wl["gt"]),
+            "reference_seconds": dt, "reference_threads": th}
+
+
+def measure_config1(device, steps, warmup):
+    """Configuration 1 (100k x 200 L2, K = 10, L = 100, 1,000 queries, its
+    seeded data and graph): the batched search on the device and through the
+    C ABI with host buffers, the plain one-launch-per-query path, the
+    reference's -Ofast search on the host cores, id parity with the
+    parity-built reference and recall@10 of both against float64 brute force.
+    Its 80 MB base fits in the 126 MB L2, so this leg is L2-resident and not
+    an HBM roofline case."""
+    import torch
+    from oracle import oracle as O
+    from scattersearch_b200 import ANNSearch, datasets, graph
+    t0 = time.time()
+    w = datasets.config(1)
+    X = torch.from_numpy(w.base).to(device)
+    adj, ep = graph.build_graph(X, R=w.graph_R, knn_k=w.graph_knn, device=device)
+    del X
+    torch.cuda.empty_cache()
+    K, L = w.K, w.L_list[0]
+    gt, _ = O.bruteforce_f64(w.base, w.queries, 10, w.metric, nthreads=cpu_threads())
+    log(f"config 1 setup {time.time() - t0:.1f}s")
+    nq, dim = w.queries.shape
+    idx = ANNSearch(dim, w.base.shape[0], w.base, w.metric)
+    idx.SetGraph(adj, ep)
+    Qd = torch.from_numpy(w.queries).to(device)
+    ids_d = torch.empty((nq, K), dtype=torch.int32, device=device)
+    st = torch.cuda.current_stream()
+    for _ in range(warmup):
+        idx.search_batch_device(Qd, nq, ids_d, None, K=K, L=L, stream=st.cuda_stream)
+    torch.cuda.synchronize()
+    evs = []
+    for _ in range(steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        idx.search_batch_device(Qd, nq, ids_d, None, K=K, L=L, stream=st.cuda_stream)
+        b.record(st)
+        evs.append((a, b))
+    torch.cuda.synchronize()
+    dev_ms = [a.elapsed_time(b) for a, b in evs]
+    ids = ids_d.cpu().numpy().view(np.uint32)
+    e2e = []
+    for i in range(warmup + steps):
+        t1 = time.perf_counter()
+        h_ids, _ = idx.search_batch(w.queries, K, L)
+        if i >= warmup:
+            e2e.append(time.perf_counter() - t1)
+    t1 = time.perf_counter()
+    plain = np.stack([idx.search(w.queries[i], K, L)[0] for i in range(nq)])
+    plain_s = time.perf_counter() - t1
+    idx.close()
+    out = {"workload": "100kx200 L2 (10-component mixture, L2-normalised), NSG R<=32, K=10, "
+                       "L=100, 1000 queries; base fits in L2",
+           "device_qps": nq * steps / (sum(dev_ms) / 1e3), "ms_per_batch": float(np.mean(dev_ms)),
+           "e2e_qps": nq * steps / sum(e2e), "plain_gpu_qps": nq / plain_s,
+           "ids_equal_plain_e2e_device": bool(np.array_equal(plain, ids)
+                                              and np.array_equal(h_ids, ids)),
+           "recall@10_gpu_vs_fp64": O.recall(ids, gt)}
+    th = cpu_threads()
+    if O.have_reference(fast=True):
+        with stdout_to_stderr():
+            fast = O.RefIndex(w.base, w.metric, adj, ep, fast=True)
+            fast.search(w.queries, K, L, nthreads=th)
+            reps, t1 = 0, time.perf_counter()
+            while reps < 3 or time.perf_counter() - t1 < 2.0:
+                fast.search(w.queries, K, L, nthreads=th)
+                reps += 1
+            out["reference_cpu_qps"] = nq * reps / (time.perf_counter() - t1)
+            out["reference_cpu"] = f"-Ofast SearchArraySimulation, OpenMP over queries, {th} threads"
+            fast.close()
+            ref = O.RefIndex(w.base, w.metric, adj, ep)
+            r_ids = ref.search(w.queries, K, L, nthreads=th)
+            ref.close()
+        tie = O.init_ties(w.base, adj, ep, w.queries, L, w.metric)
+        same = (r_ids == ids).all(1)
+        out.update({"parity_reference": "oracle/_ref/libssref.so (parity build)",
+                    "init_tie_queries": int(tie.sum()),
+                    "ids_equal_fraction": float(same.mean()),
+                    "ids_equal_fraction_excluding_init_ties": float(same[~tie].mean()),
+                    "recall@10_reference_vs_fp64": O.recall(r_ids, gt)})
+    log("config 1: " + ", ".join(f"{k} {v}" for k, v in out.items() if k != "workload"))
+    return out
+
+
+def measure_scatter_reference(idx, wl, device, nq=300, widths=(4, 8)):
+    """ScatterSearch's intra-query search, one query at a time, next to the
+    reference's own on the same queries (the tests/parallel_search.cpp:76-95
+    pattern: queries run serially, T threads each).  With election and early
+    termination at K = 100 and the bench's L; without it at L = K = 100, the
+    only pool size the reference's final merge keeps in bounds
+    (src/annsearch.cpp:651-657).  GPU latency: CUDA events around one
+    single-query launch; reference latency: host wall time per query."""
+    import torch
+    from oracle import oracle as O
+    K, L = wl["K"], wl["L"]
+    Q = wl["queries"][:nq]
+    gt = wl["gt"][:nq]
+    Qd = wl["Q"][:nq]
+    st = torch.cuda.current_stream()
+    ids = torch.empty((1, K), dtype=torch.int32, device=device)
+    ref = O.RefIndex(wl["w"].base, wl["metric"], wl["adj"], wl["ep"], fast=True) \
+        if O.have_reference(fast=True) else None
+    rows = []
+    for et, l_run in ((True, L), (False, K)):
+        for W in widths:
+            lat, got = [], []
+            for i in range(nq):
+                run = lambda: idx.search_scatter_device(Qd[i:i + 1], 1, K, l_run, W, ids,
+                                                        early_termination=et, seed=i + 1,
+                                                        stream=st.cuda_stream)
+                if i < 3:
+                    run()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(st)
+                run()
+                b.record(st)
+                b.synchronize()
+                lat.append(a.elapsed_time(b))
+                got.append(ids.cpu().numpy().view(np.uint32)[0].copy())
+            row = {"form": "WithET" if et else "plain", "T": W, "K": K, "L": l_run,
+                   "gpu": {"recall@10": recall_at_10(np.stack(got), gt),
+                           "p50_ms": float(np.percentile(lat, 50)),
+                           "p99_ms": float(np.percentile(lat, 99))}}
+            if ref is not None:
+                with stdout_to_stderr():
+                    if et:
+                        r_ids, r_lat, r_st = ref.search_et(Q, K, l_run, W, seed=7, with_stats=True)
+                    else:
+                        r_ids, r_lat, r_st = ref.search_scatter(Q, K, W, seed=7)
+                row["reference"] = {"recall@10": recall_at_10(r_ids, gt),
+                                    "p50_ms": float(np.percentile(r_lat, 50)) / 1e3,
+                                    "p99_ms": float(np.percentile(r_lat, 99)) / 1e3,
+                                    "dist_comps_per_query": float(r_st[0]) / nq}
+            rows.append(row)
+            log(f"scatter {row['form']} T={W} L={l_run}: gpu {row['gpu']} "
+                f"reference {row.get('reference')}")
+    if ref is not None:
+        ref.close()
+    return {"queries": nq, "timing": "per query: CUDA events (GPU), host wall time (reference "
+            "-Ofast build, OpenMP threads = T)", "rows": rows}
 
 
 def measure_intra_latency(idx, wl, L, device, batches=(1, 4, 16), widths=(4, 8, 16), reps=10):
@@ -555,7 +764,12 @@ def run_ours(args):
 
     # launch layout (teams per CTA, visited-table size) tuned on a sample
     from scattersearch_b200 import autotune
-    tune = autotune.autotune(idx, wl["Q"], K, L, reps=2, path=None)
+    if args.layout:
+        wpb, hc, sh, rows = (int(x) for x in args.layout.split(","))
+        tune = {"warps_per_block": wpb, "hash_cap": hc, "shared_stages": sh, "stage_rows": rows,
+                "table": []}
+    else:
+        tune = autotune.autotune(idx, wl["Q"], K, L, reps=2, path=None)
     for r in sorted(tune["table"], key=lambda r: r["ms"])[:6]:
         log(f"  layout {r}")
     log(f"tuned: {tune['warps_per_block']} teams per CTA, {tune['shared_stages']} shared stages "
@@ -658,10 +872,18 @@ def run_ours(args):
     plain_qps = ns / plain_s
     plain_same = bool(np.array_equal(plain_ids, ids_np[:ns]))
 
-    online = None if args.no_online else measure_online(idx, wl, L)
-    intra = None if args.no_online else measure_intra_latency(idx, wl, L, device)
+    # legs beside the headline, at N = 1 only (setup and host work that would
+    # hold the other ranks' GPUs)
+    solo = d.rank == 0 and d.world == 1
+    wl["L"] = L
+    parity = parity_record(wl, ids_np, L) if solo and not args.no_parity else None
+    online = measure_online(idx, wl) if solo and not args.no_online else None
+    intra = measure_intra_latency(idx, wl, L, device) if solo and not args.no_online else None
+    scatter = measure_scatter_reference(idx, wl, device) if solo and not args.no_online else None
     idx.set_tuning(tune["warps_per_block"], tune["hash_cap"], 0, tune["shared_stages"],
                    tune["stage_rows"])
+    config1 = measure_config1(device, args.steps, args.warmup) \
+        if solo and not args.no_config1 and args.workload == "cfg3" and args.scale == 1.0 else None
 
     peak, peak_kind = measured_hbm_peak()
     traffic, traffic_src = profiled_traffic(args.workload, L, nq)
@@ -699,8 +921,11 @@ def run_ours(args):
                      "distance_evals_per_s": float(ndc.sum()) / mean_step_s,
                      "device_evals_per_query": float(ndc_dev.mean()),
                      "device_row_gbps": device_bytes_per_step / mean_step_s / 1e9},
+        "parity": parity,
         "online": online,
         "intra_latency": intra,
+        "scatter_vs_reference": scatter,
+        "config1": config1,
         "gpu_launches": args.steps,
         "launch": "one CUDA graph per step (queue reset, status reset, search kernel)",
         "clocks": clocks,

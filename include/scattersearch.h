@@ -189,8 +189,11 @@ int ss_batch_status(ss_index *h, uint32_t *failed_queries);
  *     overlaps on the GPU (other streams, other threads) race and must be
  *     serialised by the caller.
  *   - Enqueued on `stream` (a cudaStream_t, NULL for the legacy default
- *     stream); the call returns once the search has finished, reporting
- *     SS_ERR_SEARCH_LIMIT if any query hit the hop limit. */
+ *     stream); the call returns once the search has finished.  Failed
+ *     queries are reported as ss_search_batch reports them:
+ *     SS_ERR_SEARCH_LIMIT for the hop limit or a full visited table,
+ *     SS_ERR_TIMEOUT for a row-copy wait that ran out, SS_ERR_INVALID_ARGUMENT
+ *     otherwise; ss_last_error names the count and the first failed query. */
 #define SS_NOALLOC_MAX_QUERIES 65536
 #define SS_NOALLOC_SCRATCH_BYTES (256u + 4u * SS_NOALLOC_MAX_QUERIES)
 int ss_search_batch_noalloc(ss_index *h, const float *queries, uint32_t nq, int K, int L,

@@ -63,6 +63,10 @@ def _lib_oracle() -> ctypes.CDLL:
         lib.sso_bruteforce.argtypes = [
             _c_f32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, _c_f32p, ctypes.c_uint32,
             ctypes.c_int, _c_u32p, _c_f32p, ctypes.c_int]
+        lib.sso_bruteforce_f64.restype = ctypes.c_int
+        lib.sso_bruteforce_f64.argtypes = [
+            _c_f32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, _c_f32p, ctypes.c_uint32,
+            ctypes.c_int, _c_u32p, _c_f64p, ctypes.c_int]
         _libs["oracle"] = lib
     return _libs["oracle"]
 
@@ -93,7 +97,12 @@ def _lib_ref(fast: bool = False) -> ctypes.CDLL:
                                            ctypes.c_int, _c_u32p, ctypes.c_int]
         lib.ssref_search_et.restype = ctypes.c_int
         lib.ssref_search_et.argtypes = [ctypes.c_void_p, _c_f32p, ctypes.c_uint, ctypes.c_int,
-                                        ctypes.c_int, ctypes.c_int, ctypes.c_uint, _c_u32p, _c_f64p]
+                                        ctypes.c_int, ctypes.c_int, ctypes.c_uint, _c_u32p, _c_f64p,
+                                        _c_f64p]
+        lib.ssref_search_scatter.restype = ctypes.c_int
+        lib.ssref_search_scatter.argtypes = [ctypes.c_void_p, _c_f32p, ctypes.c_uint, ctypes.c_int,
+                                             ctypes.c_int, ctypes.c_int, ctypes.c_uint, _c_u32p,
+                                             _c_f64p, _c_f64p]
         _libs[key] = lib
     return _libs[key]
 
@@ -158,6 +167,46 @@ def bruteforce(base, queries, k: int, metric: int, nthreads: int | None = None):
     return ids, dists
 
 
+def bruteforce_f64(base, queries, k: int, metric: int, nthreads: int | None = None):
+    """Exact k-NN with float64 distances (ties by smaller id): the ground
+    truth recall is pinned against.  Returns (ids uint32, dists float64)."""
+    base, queries = _f32(base), _f32(queries)
+    nq = queries.shape[0]
+    ids = np.zeros((nq, k), dtype=np.uint32)
+    dists = np.zeros((nq, k), dtype=np.float64)
+    _lib_oracle().sso_bruteforce_f64(_ptr(base, _c_f32p), base.shape[0], base.shape[1], metric,
+                                     _ptr(queries, _c_f32p), nq, k, _ptr(ids, _c_u32p),
+                                     _ptr(dists, _c_f64p), nthreads or os.cpu_count() or 1)
+    return ids, dists
+
+
+def recall(ids, gt, k: int = 10) -> float:
+    """Mean fraction of the first k ids of each row found among gt's first k
+    (the reference drivers' recall@K, tests/search.cpp:90-104)."""
+    ids = np.asarray(ids)[:, :k].astype(np.int64)
+    gt = np.asarray(gt)[:, :k].astype(np.int64)
+    hits = sum(int(np.isin(ids[i], gt[i]).sum()) for i in range(len(ids)))
+    return hits / float(k * len(ids))
+
+
+def init_ties(base, adj, ep: int, queries, L: int, metric: int):
+    """Per query: True when the initial pool (the first min(L, deg(ep))
+    neighbours of the entry point) holds two distinct ids at exactly the same
+    distance.  The reference orders that pool with std::sort, which is not
+    stable (src/annsearch.cpp:215), so its order of such ties is
+    implementation-defined."""
+    adj = _u32(adj)
+    row = adj[ep][adj[ep] != NONE_ID][:L]
+    uniq = np.unique(row)
+    out = np.zeros(len(queries), dtype=bool)
+    if len(uniq) < 2:
+        return out
+    for i, q in enumerate(_f32(queries)):
+        d = np.array([distance(base[j], q, metric) for j in uniq], dtype=np.float32)
+        out[i] = len(np.unique(d)) != len(d)
+    return out
+
+
 class RefIndex:
     """The reference's ANNSearch engine, compiled in place (oracle/_ref)."""
 
@@ -198,15 +247,36 @@ class RefIndex:
             raise ValueError("reference search rejected its arguments")
         return ids
 
-    def search_et(self, queries, K: int, L: int, nthreads: int, seed: int = 1):
+    def search_et(self, queries, K: int, L: int, nthreads: int, seed: int = 1,
+                  with_stats: bool = False):
+        """MultiThreadSearchArraySimulationWithET, queries one at a time:
+        (ids, per-query microseconds[, engine counters dist_comps,
+        max_dist_comps, hop_count summed over the queries])."""
         queries = _f32(queries)
         ids = np.zeros((queries.shape[0], K), dtype=np.uint32)
         lat = np.zeros(queries.shape[0], dtype=np.float64)
+        st = np.zeros(3, dtype=np.float64)
         rc = self._lib.ssref_search_et(self._h, _ptr(queries, _c_f32p), queries.shape[0], K, L,
-                                       nthreads, seed, _ptr(ids, _c_u32p), _ptr(lat, _c_f64p))
+                                       nthreads, seed, _ptr(ids, _c_u32p), _ptr(lat, _c_f64p),
+                                       _ptr(st, _c_f64p))
         if rc != 0:
             raise ValueError("reference ET search rejected its arguments")
-        return ids, lat
+        return (ids, lat, st) if with_stats else (ids, lat)
+
+    def search_scatter(self, queries, K: int, nthreads: int, seed: int = 1):
+        """MultiThreadSearchArraySimulation with L = K (the only pool size its
+        final merge keeps in bounds), queries one at a time: (ids, per-query
+        microseconds, engine counters dist_comps, max_dist_comps, hop_count)."""
+        queries = _f32(queries)
+        ids = np.zeros((queries.shape[0], K), dtype=np.uint32)
+        lat = np.zeros(queries.shape[0], dtype=np.float64)
+        st = np.zeros(3, dtype=np.float64)
+        rc = self._lib.ssref_search_scatter(self._h, _ptr(queries, _c_f32p), queries.shape[0], K,
+                                            K, nthreads, seed, _ptr(ids, _c_u32p),
+                                            _ptr(lat, _c_f64p), _ptr(st, _c_f64p))
+        if rc != 0:
+            raise ValueError("reference scatter search rejected its arguments")
+        return ids, lat, st
 
 
 def ref_distance(a, b, metric: int) -> float:

@@ -7,6 +7,7 @@
 //   ANNSearch ctor / metric dispatch         src/annsearch.cpp:11-58
 //   ANNSearch::LoadGraph (.nsg reader)       src/annsearch.cpp:64-80
 //   ANNSearch::SearchArraySimulation         src/annsearch.cpp:182-259
+//   ANNSearch::MultiThreadSearchArraySimulation        src/annsearch.cpp:532-699
 //   ANNSearch::MultiThreadSearchArraySimulationWithET  src/annsearch.cpp:839-1025
 //   distance_l2sqr_avx / distance_ip_avx     src/distance.cpp:19-56, 115-149
 //
@@ -22,7 +23,29 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <new>
 #include <vector>
+
+// Every allocation made by code in this library gets 64 bytes of slack past
+// its end.  MultiThreadSearchArraySimulation merges the threads' pools into
+// a vector of K entries with InsertIntoPool(final_result.data(), K, nn)
+// (src/annsearch.cpp:660-666), and InsertIntoPool stores a candidate worse
+// than all K at addr[K] (include/util.h:52-55): one 12-byte Neighbor past the
+// vector.  The slack keeps that store inside the allocation instead of
+// corrupting the heap; the reference's code is unchanged.  oracle/Makefile
+// links with -Bsymbolic-functions so the reference's code in this library
+// binds to these definitions.  They call malloc/free directly, so memory
+// allocated here and freed elsewhere (or the reverse) stays compatible.
+void* operator new(std::size_t n) {
+  void* p = std::malloc(n + 64);
+  if (!p) throw std::bad_alloc();
+  return p;
+}
+void* operator new[](std::size_t n) { return operator new(n); }
+void operator delete(void* p) noexcept { std::free(p); }
+void operator delete[](void* p) noexcept { std::free(p); }
+void operator delete(void* p, std::size_t) noexcept { std::free(p); }
+void operator delete[](void* p, std::size_t) noexcept { std::free(p); }
 
 namespace {
 
@@ -129,15 +152,19 @@ int ssref_search_batch(void* p, const float* queries, unsigned nq, int K, int L,
 // pattern).  Its election starts from best_dist = 1000 (annsearch.cpp:850),
 // so it is only meaningful for inner product / unit-norm data; L >= K and
 // every graph row non-empty are required by its indexing.  lat_us: per-query
-// wall time in microseconds (may be null).
+// wall time in microseconds (may be null); stats (may be null): the engine's
+// counters after the run, [0] dist_comps, [1] max_dist_comps, [2] hop_count.
 int ssref_search_et(void* p, const float* queries, unsigned nq, int K, int L, int nthreads,
-                    unsigned seed, uint32_t* ids, double* lat_us) {
+                    unsigned seed, uint32_t* ids, double* lat_us, double* stats) {
   auto* h = static_cast<RefIndex*>(p);
   if (K > L || K <= 0) return -1;
   std::vector<float> q = padded_copy(queries, (size_t)nq * h->dim);
   boost::dynamic_bitset<> flags(h->n, 0);
   std::vector<unsigned> tmp(K);
   srand(seed);
+  h->eng->dist_comps = 0;
+  h->eng->max_dist_comps = 0;
+  h->eng->hop_count = 0;
   for (unsigned i = 0; i < nq; ++i) {
     double t0 = omp_get_wtime();
     h->eng->MultiThreadSearchArraySimulationWithET(q.data() + (size_t)i * h->dim, i, K, L, nthreads,
@@ -145,6 +172,48 @@ int ssref_search_et(void* p, const float* queries, unsigned nq, int K, int L, in
     double t1 = omp_get_wtime();
     if (lat_us) lat_us[i] = (t1 - t0) * 1e6;
     for (int j = 0; j < K; ++j) ids[(size_t)i * K + j] = tmp[j];
+  }
+  if (stats) {
+    stats[0] = (double)h->eng->dist_comps;
+    stats[1] = (double)h->eng->max_dist_comps;
+    stats[2] = (double)h->eng->hop_count;
+  }
+  return 0;
+}
+
+// MultiThreadSearchArraySimulation (src/annsearch.cpp:532-699), the form
+// without election, queries one after another with `nthreads` intra-query
+// threads.  Its final merge first copies L entries into a vector of K
+// (annsearch.cpp:651-657), so only L == K stays near that vector (its one
+// store past the end is absorbed by the allocation slack above); other
+// values are refused here.  Every thread's random padding walks forward past
+// visited ids without a bound (:568-574), which the pad ids never reach in
+// practice on graphs far larger than L x nthreads.  Per-query wall time in
+// microseconds to lat_us (may be null); the engine's counters are summed
+// into stats[0..2] = dist_comps, max_dist_comps, hop_count (may be null).
+int ssref_search_scatter(void* p, const float* queries, unsigned nq, int K, int L, int nthreads,
+                         unsigned seed, uint32_t* ids, double* lat_us, double* stats) {
+  auto* h = static_cast<RefIndex*>(p);
+  if (K <= 0 || L != K) return -1;
+  std::vector<float> q = padded_copy(queries, (size_t)nq * h->dim);
+  boost::dynamic_bitset<> flags(h->n, 0);
+  std::vector<unsigned> tmp(K);
+  srand(seed);
+  h->eng->dist_comps = 0;
+  h->eng->max_dist_comps = 0;
+  h->eng->hop_count = 0;
+  for (unsigned i = 0; i < nq; ++i) {
+    double t0 = omp_get_wtime();
+    h->eng->MultiThreadSearchArraySimulation(q.data() + (size_t)i * h->dim, i, K, L, nthreads,
+                                             flags, tmp);
+    double t1 = omp_get_wtime();
+    if (lat_us) lat_us[i] = (t1 - t0) * 1e6;
+    for (int j = 0; j < K; ++j) ids[(size_t)i * K + j] = tmp[j];
+  }
+  if (stats) {
+    stats[0] = (double)h->eng->dist_comps;
+    stats[1] = (double)h->eng->max_dist_comps;
+    stats[2] = (double)h->eng->hop_count;
   }
   return 0;
 }

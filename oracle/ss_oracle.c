@@ -246,3 +246,50 @@ int sso_bruteforce(const float *base, uint32_t n, uint32_t dim, int metric, cons
   }
   return 0;
 }
+
+/* Exact k-NN in double precision: the float64 ground truth the benchmark
+ * configurations pin recall against (L2: sum of squared differences; inner
+ * product: minus the dot product; both accumulated in double).  Ties are
+ * broken by the smaller id.  ids: nq x k (SSO_NONE past n). */
+int sso_bruteforce_f64(const float *base, uint32_t n, uint32_t dim, int metric,
+                       const float *queries, uint32_t nq, int k, uint32_t *ids, double *dists,
+                       int nthreads) {
+  if (k <= 0) return -1;
+#pragma omp parallel for num_threads(nthreads > 0 ? nthreads : 1) schedule(dynamic, 1)
+  for (long i = 0; i < (long)nq; ++i) {
+    double *bd = (double *)malloc(sizeof(double) * (size_t)k);
+    uint32_t *bi = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)k);
+    int cnt = 0;
+    const float *q = queries + (size_t)i * dim;
+    for (uint32_t j = 0; j < n; ++j) {
+      const float *x = base + (size_t)j * dim;
+      double s = 0.0;
+      if (metric == SSO_L2) {
+        for (uint32_t t = 0; t < dim; ++t) {
+          const double d = (double)q[t] - (double)x[t];
+          s += d * d;
+        }
+      } else {
+        for (uint32_t t = 0; t < dim; ++t) s += (double)q[t] * (double)x[t];
+        s = -s;
+      }
+      /* j ascends, so an equal distance never displaces an earlier id */
+      if (cnt == k && s >= bd[k - 1]) continue;
+      int p = cnt < k ? cnt++ : k - 1;
+      while (p > 0 && bd[p - 1] > s) {
+        bd[p] = bd[p - 1];
+        bi[p] = bi[p - 1];
+        --p;
+      }
+      bd[p] = s;
+      bi[p] = j;
+    }
+    for (int t = 0; t < k; ++t) {
+      ids[(size_t)i * k + t] = t < cnt ? bi[t] : SSO_NONE;
+      if (dists) dists[(size_t)i * k + t] = t < cnt ? bd[t] : 0.0;
+    }
+    free(bd);
+    free(bi);
+  }
+  return 0;
+}

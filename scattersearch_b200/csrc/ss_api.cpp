@@ -215,23 +215,40 @@ int check_search_args(ss_index *h, int K, int L) {
   return SS_OK;
 }
 
+// Error for a batch from its counts of failed queries per status code
+// (counts[c] = queries with status c, 1 <= c < kStatusKinds) and the index
+// of the first failed query.  The most severe kind present decides the code.
+int status_counts_to_error(ss_index *h, const uint32_t *counts, uint32_t first) {
+  const uint32_t bad = counts[ssb::kStatusBadArgs], hop = counts[ssb::kStatusHopLimit];
+  const uint32_t full = counts[ssb::kStatusVisitedFull];
+  const uint32_t timeout = counts[ssb::kStatusStageTimeout];
+  if (timeout)
+    return set_err(h, SS_ERR_TIMEOUT,
+                   "%u queries gave up waiting for their row copies (first failed query: %u); "
+                   "results are invalid", timeout, first);
+  if (hop)
+    return set_err(h, SS_ERR_SEARCH_LIMIT, "%u queries hit the hop limit (first failed query: %u)",
+                   hop, first);
+  if (full)
+    return set_err(h, SS_ERR_SEARCH_LIMIT,
+                   "%u queries overflowed the visited table (first failed query: %u)", full, first);
+  if (bad)
+    return set_err(h, SS_ERR_INVALID_ARGUMENT, "%u queries had invalid K/L (first failed query: %u)",
+                   bad, first);
+  return SS_OK;
+}
+
 int status_to_error(ss_index *h, const int32_t *st, uint32_t nq) {
-  uint32_t bad = 0, hop = 0, full = 0, first = 0;
+  uint32_t counts[ssb::kStatusKinds] = {};
+  uint32_t first = 0, failed = 0;
   for (uint32_t i = 0; i < nq; ++i) {
     if (st[i] != ssb::kStatusOk) {
-      if (bad == 0) first = i;
-      ++bad;
-      if (st[i] == ssb::kStatusHopLimit) ++hop;
-      if (st[i] == ssb::kStatusVisitedFull) ++full;
+      if (failed++ == 0) first = i;
+      // an unknown code counts as invalid arguments
+      ++counts[st[i] > 0 && st[i] < ssb::kStatusKinds ? st[i] : ssb::kStatusBadArgs];
     }
   }
-  if (!bad) return SS_OK;
-  if (hop)
-    return set_err(h, SS_ERR_SEARCH_LIMIT, "%u queries hit the hop limit (first: %u)", hop, first);
-  if (full)
-    return set_err(h, SS_ERR_SEARCH_LIMIT, "%u queries overflowed the visited table (first: %u)",
-                   full, first);
-  return set_err(h, SS_ERR_INVALID_ARGUMENT, "%u queries had invalid K/L (first: %u)", bad, first);
+  return failed ? status_counts_to_error(h, counts, first) : SS_OK;
 }
 
 // Persistent grid size for the warp kernel: every SM filled, never more
@@ -1156,18 +1173,24 @@ int ss_search_batch_noalloc(ss_index *h, const float *queries, uint32_t nq, int 
   a.status = sc.status;
   a.work_counter = sc.counter;
   a.max_hops = h->n + 1;
-  // The scratch keeps whatever the previous call left: clear the queue head,
-  // the failure count and this batch's status words.
-  SS_CUDA(h, cudaMemsetAsync(sc.counter, 0, 2 * sizeof(uint32_t), st), "scratch reset");
+  // The scratch keeps whatever the previous call left: reset the queue head,
+  // the failure counters (first failed index to 0xFFFFFFFF, counts to 0) and
+  // this batch's status words.
+  SS_CUDA(h, cudaMemsetAsync(sc.counter, 0, sizeof(uint32_t), st), "scratch reset");
+  SS_CUDA(h, cudaMemsetAsync(sc.failed, 0xFF, sizeof(uint32_t), st), "scratch reset");
+  SS_CUDA(h, cudaMemsetAsync(sc.failed + 1, 0, (ssb::kStatusKinds - 1) * sizeof(uint32_t), st),
+          "scratch reset");
   SS_CUDA(h, cudaMemsetAsync(sc.status, 0, (size_t)nq * 4, st), "scratch reset");
   SS_CUDA(h, ssb::launch_warp_search(g, a, plan, wpb, blocks, st), "search launch");
   SS_CUDA(h, ssb::launch_count_failed(sc.status, nq, sc.failed, st), "status count launch");
-  uint32_t failed = 0;
-  SS_CUDA(h, cudaMemcpyAsync(&failed, sc.failed, sizeof(failed), cudaMemcpyDeviceToHost, st),
+  uint32_t failed[ssb::kStatusKinds] = {};
+  SS_CUDA(h, cudaMemcpyAsync(failed, sc.failed, sizeof(failed), cudaMemcpyDeviceToHost, st),
           "status count download");
   SS_CUDA(h, cudaStreamSynchronize(st), "allocation-free search");
-  if (failed) return set_err(h, SS_ERR_SEARCH_LIMIT, "%u queries hit the hop limit", failed);
-  return SS_OK;
+  // failed[0] holds the first failed index; the per-code counts follow it
+  const uint32_t first = failed[0];
+  failed[0] = 0;
+  return first == 0xFFFFFFFFu ? SS_OK : status_counts_to_error(h, failed, first);
 }
 
 static int intra_common(ss_index *h, const float *queries, uint32_t nq, int K, int L, int W,

@@ -64,7 +64,8 @@ enum : int32_t {
   kStatusBadArgs = 1,
   kStatusHopLimit = 2,
   kStatusVisitedFull = 3,
-  kStatusStageTimeout = 4  // a shared-memory row stage was not filled within its wait limit
+  kStatusStageTimeout = 4,  // a shared-memory row stage was not filled within its wait limit
+  kStatusKinds = 5          // number of status codes
 };
 
 // Plans shared memory for a warp-per-query launch.
@@ -104,14 +105,17 @@ constexpr uint32_t kNoallocMaxQueries = 65536;
 constexpr size_t kNoallocScratchBytes = 256 + size_t(4) * kNoallocMaxQueries;
 struct NoallocScratch {
   uint32_t *counter;  // persistent work-queue head
-  uint32_t *failed;   // count of queries with a nonzero status
+  uint32_t *failed;   // kStatusKinds words: [c] = queries with status c (c >= 1),
+                      // [0] = index of the first failed query (0xFFFFFFFF: none)
   int32_t *status;    // kNoallocMaxQueries entries
 };
 // Device addresses of the scratch on the current device.  The first call on
 // a device resolves them (cudaGetSymbolAddress); later calls only read a
 // cache.
 cudaError_t noalloc_scratch(NoallocScratch *out);
-// Adds the number of nonzero status[0..nq) to *failed.
+// Counts the failed queries of status[0..nq) per status code into
+// failed[1..kStatusKinds) and lowers failed[0] to the smallest failed index
+// (failed[] as in NoallocScratch, set up by the caller beforehand).
 cudaError_t launch_count_failed(const int32_t *status, uint32_t nq, uint32_t *failed,
                                 cudaStream_t stream);
 

@@ -655,7 +655,13 @@ __device__ __forceinline__ void accepted_positions(const WarpSmem &s, int na, in
 // Step 4 of a hop: candidates cid/ckey[0..nc) (adjacency order) with key
 // below the hop's threshold are accepted, in order, into ak/aid/acle with
 // their pool rank (entries <= key).  With check_dups, a candidate whose id is
-// already in the pool under the same key is dropped.  Returns the count.
+// already in the pool under the same key is dropped, and so is one whose id
+// was accepted from an earlier 32-id chunk of the same row: a table that
+// forgets can lose an id recorded earlier in the same hop, so a row that
+// repeats an id across chunks would otherwise offer it twice, where the
+// reference's visited flags skip the second occurrence (annsearch.cpp:229-231).
+// Both copies have the same key, so the first one is accepted iff the second
+// would be.  Returns the count.
 template <int RCH>
 __device__ __forceinline__ int accept_candidates(const WarpSmem &s, int nc, int size, uint32_t thr,
                                                  bool check_dups, int lane) {
@@ -669,6 +675,7 @@ __device__ __forceinline__ int accept_candidates(const WarpSmem &s, int nc, int 
     bool acc = e < nc && key < thr;
     int cle = 0;
     uint32_t id = 0;
+    if (c > 0 && check_dups) __syncwarp();  // earlier chunks' aid/ak stores are visible
     if (acc) {
       id = s.cid[e];
       cle = count_le_bf(s.pk, size, top, key);
@@ -678,6 +685,9 @@ __device__ __forceinline__ int accept_candidates(const WarpSmem &s, int nc, int 
             acc = false;
             break;
           }
+        }
+        for (int j = 0; c > 0 && acc && j < na; ++j) {
+          if (s.aid[j] == id && s.ak[j] == key) acc = false;
         }
       }
     }
@@ -2114,26 +2124,44 @@ cudaError_t launch_intra_search(const GraphView &g, const BatchArgs &a, const Sm
 // ------------------------------------------------ allocation-free launch ---
 // Scratch of ss_search_batch_noalloc: one file-scope device array per GPU
 // that loads the library, held until the process exits.  Layout (4-byte
-// words): [0] work-queue head, [1] failed-query count, [64, 64 + max
-// queries) per-query status.  Every call shares it, so calls whose work
-// overlaps on the GPU race; each call clears the parts it uses before its
-// search runs.
+// words): [0] work-queue head, [1] first failed query, [2, 1 + kStatusKinds)
+// failed queries per status code, [64, 64 + max queries) per-query status.
+// Every call shares it, so calls whose work overlaps on the GPU race; each
+// call resets the parts it uses before its search runs.
 namespace {
 constexpr size_t kNoallocWords = kNoallocScratchBytes / 4;
 constexpr size_t kNoallocStatusAt = 64;
 static_assert(kNoallocStatusAt + kNoallocMaxQueries <= kNoallocWords,
               "scratch too small for its status words");
+static_assert(1 + kStatusKinds <= kNoallocStatusAt, "counters overlap the status words");
 
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoallocWords];
 
-// Counts the nonzero statuses of a batch into *failed (zeroed beforehand).
+// Counts the failed queries of a batch per status code into
+// failed[1..kStatusKinds) (zeroed beforehand) and lowers failed[0] (set to
+// 0xFFFFFFFF beforehand) to the smallest failed query index.  A code outside
+// the known ones counts as invalid arguments.
 __global__ void __launch_bounds__(256) count_failed_kernel(const int32_t *status, uint32_t nq,
                                                            uint32_t *failed) {
-  uint32_t c = 0;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x)
-    c += status[i] != kStatusOk;
-  c = __reduce_add_sync(kFull, c);
-  if ((threadIdx.x & 31) == 0 && c) atomicAdd(failed, c);
+  uint32_t c[kStatusKinds] = {};
+  uint32_t first = 0xFFFFFFFFu;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) {
+    const int32_t s = status[i];
+    if (s != kStatusOk) {
+      first = min(first, i);
+#pragma unroll
+      for (int k = 1; k < kStatusKinds; ++k)
+        c[k] += (s == k) || (k == kStatusBadArgs && (s < 0 || s >= kStatusKinds));
+    }
+  }
+  first = __reduce_min_sync(kFull, first);
+  const bool lead = (threadIdx.x & 31) == 0;
+  if (lead && first != 0xFFFFFFFFu) atomicMin(failed, first);
+#pragma unroll
+  for (int k = 1; k < kStatusKinds; ++k) {
+    const uint32_t t = __reduce_add_sync(kFull, c[k]);
+    if (lead && t) atomicAdd(failed + k, t);
+  }
 }
 }  // namespace
 

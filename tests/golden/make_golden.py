@@ -1,6 +1,6 @@
 """Generates the golden fixtures in this directory from the REFERENCE itself.
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle REF=<reference source tree> && python tests/golden/make_golden.py
 
 Runs only where the reference sources were available to build
 oracle/_ref/libssref.so (the reference's own ANNSearch, compiled in place with
@@ -60,8 +60,8 @@ def make_search_fixture(name, base, queries, metric, R, cases, knn_k=None):
 
 def main():
     if not O.have_reference():
-        raise SystemExit("oracle/_ref/libssref.so is missing: run `make -C oracle` with the "
-                         "reference sources present")
+        raise SystemExit("oracle/_ref/libssref.so is missing: run "
+                         "`make -C oracle REF=<reference source tree>`")
     rng = np.random.default_rng(20240601)
 
     # Gaussian mixture, L2, dim 64 (an even number of 8-blocks)

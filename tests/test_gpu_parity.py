@@ -179,6 +179,67 @@ def test_visited_spill_to_global_bitset(oracle_lib):
     idx.close()
 
 
+def _rows_repeating_across_chunks(adj, seed, repeats=8):
+    """Every row rewritten to hold at least 33 ids, the last `repeats` of
+    them copies of ids from its first 32 (so each row repeats ids in its
+    second 32-id chunk); rows shorter than 32 are first filled up with
+    random other ids."""
+    rng = np.random.default_rng(seed)
+    n, width = adj.shape
+    out = np.full((n, max(width, 64)), NONE_ID, dtype=np.uint32)
+    for i in range(n):
+        nb = adj[i][adj[i] != NONE_ID]
+        if len(nb) < 32:
+            extra = rng.choice(n, 64, replace=False)
+            extra = extra[~np.isin(extra, nb) & (extra != i)][:32 - len(nb)]
+            nb = np.concatenate([nb, extra.astype(np.uint32)])
+        nb = nb[:64 - repeats]
+        rep = nb[rng.choice(32, repeats, replace=False)]
+        row = np.concatenate([nb, rep])
+        out[i, :len(row)] = row
+    return out
+
+
+def test_repeated_ids_across_row_chunks(oracle_lib):
+    """Rows of 40-64 ids (two 32-id chunks) that repeat ids of the first
+    chunk in the second, searched with a visited table small enough to forget
+    ids within a hop: the second occurrence must be skipped as the
+    reference's visited flags skip it (src/annsearch.cpp:229-231), never
+    entering the pool twice."""
+    O = oracle_lib
+    X, Q, _, _ = _synthetic(64 + 77, 20000, 64, 32, 0, clusters=4)
+    from scattersearch_b200 import graph
+    adj0, ep = graph.build_graph(X, R=48, knn_k=96, device="cpu")
+    adj = _rows_repeating_across_chunks(adj0, seed=3)
+    assert ((adj != NONE_ID).sum(1) > 32).all()
+    idx = _index(X, adj, ep, 0)
+    big = _tile(Q)
+    reps = len(big) // len(Q)
+    for K, L in ((10, 100), (50, 400)):
+        o_ids, o_d, ndc, _ = O.search(X, adj, ep, 0, Q, K, L)
+        if L == 400:
+            assert ndc.max() > 1024  # far more ids than the 512-slot table holds
+        for tuning in (dict(warps_per_block=4, hash_cap=512), dict(hash_cap=512, stage_rows=12),
+                       dict()):
+            idx.set_tuning(**tuning)
+            ids, d = idx.search_batch(big, K, L)
+            assert np.array_equal(ids, np.tile(o_ids, (reps, 1))), (K, L, tuning)
+            assert _same_bits(d, np.tile(o_d, (reps, 1))), (K, L, tuning)
+            # no query's result holds an id twice unless the oracle's does
+            dup = np.array([len(set(r.tolist())) < len(r) for r in ids[:len(Q)]])
+            o_dup = np.array([len(set(r.tolist())) < len(r) for r in o_ids])
+            assert np.array_equal(dup, o_dup)
+        idx.set_tuning()
+        if O.have_reference():
+            ref = O.RefIndex(X, 0, adj, ep)
+            r_ids = ref.search(Q, K, L)
+            ref.close()
+            tie = O.init_ties(X, adj, ep, Q, L, 0)
+            same = (o_ids == r_ids).all(1)
+            assert same[~tie].all(), np.flatnonzero(~same & ~tie)
+    idx.close()
+
+
 def test_edge_cases(oracle_lib):
     O = oracle_lib
     rng = np.random.default_rng(9)
