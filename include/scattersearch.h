@@ -240,6 +240,17 @@ int ss_search_scatter_batch(ss_index *h, const float *queries, uint32_t nq, int 
                             int num_threads, int early_termination, uint64_t seed, uint32_t *ids,
                             float *dists);
 
+/* ss_search_scatter_batch that also returns the counters the reference's
+ * engine keeps for these searches (src/annsearch.cpp:683-695, :1011-1020),
+ * per query, in host arrays of nq entries (each may be NULL): distance
+ * evaluations summed over the warps (dist_comps), the most and the fewest
+ * of one warp (max_dist_comps; max / min is its ub_ratio), and expansions
+ * summed over the warps (hop_count, kept by the form without election). */
+int ss_search_scatter_batch_stats(ss_index *h, const float *queries, uint32_t nq, int K, int L,
+                                  int num_threads, int early_termination, uint64_t seed,
+                                  uint32_t *ids, float *dists, uint32_t *ndc_sum,
+                                  uint32_t *ndc_max, uint32_t *ndc_min, uint32_t *hops_sum);
+
 /* Device-pointer form (asynchronous on `stream`); ndc / hops (nq uint32,
  * may be NULL) receive each query's distance evaluations and expansions
  * summed over its warps. */

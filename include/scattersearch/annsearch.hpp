@@ -11,7 +11,15 @@
 //     error behaviour for loaders (src/util.cpp:42-47) applied to every call
 //     (its LoadGraph ignores a failed open, src/annsearch.cpp:66);
 //   * `graph` (vector<vector<unsigned>>) is not kept on the host;
-//     graph_table() copies the device adjacency out on demand.
+//     graph_table() copies the device adjacency out on demand;
+//   * the public counters follow the reference's bookkeeping: the
+//     ScatterSearch methods add their distance evaluations (dist_comps), the
+//     busiest warp's evaluations (max_dist_comps), max / min over the warps
+//     (ub_ratio) and, without election, the expansions (hop_count), as
+//     src/annsearch.cpp:634, :683-695 and :1011-1020 do; SearchArraySimulation
+//     leaves them alone, as the reference does (its increments are commented
+//     out, src/annsearch.cpp:212, :237).  The updates are serialised by a
+//     lock, where the reference's are plain racy increments.
 #ifndef SCATTERSEARCH_ANNSEARCH_HPP
 #define SCATTERSEARCH_ANNSEARCH_HPP
 
@@ -21,6 +29,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <mutex>
 #include <vector>
 
 namespace scattersearch {
@@ -158,15 +167,22 @@ class ANNSearch {
                std::vector<unsigned> &indices, const char *what) {
     if ((int)indices.size() < K) indices.resize(K);
     const uint64_t seed = (uint64_t)query_id * 0x9E3779B97F4A7C15ull + 1ull;
-    die_on_error(ss_search_scatter_batch(handle, query, 1, K, L, num_threads, et, seed,
-                                         reinterpret_cast<uint32_t *>(indices.data()), nullptr),
+    uint32_t sum = 0, most = 0, fewest = 0, hops = 0;
+    die_on_error(ss_search_scatter_batch_stats(handle, query, 1, K, L, num_threads, et, seed,
+                                               reinterpret_cast<uint32_t *>(indices.data()),
+                                               nullptr, &sum, &most, &fewest, &hops),
                  handle, what);
+    std::lock_guard<std::mutex> lk(counter_mu_);
+    dist_comps += sum;
+    max_dist_comps += most;
+    ub_ratio += fewest ? (float)most / (float)fewest : 0.f;
+    if (!et) hop_count += (int)hops;  // the election form keeps no hop count
   }
+  std::mutex counter_mu_;
 
  public:
-  // Public members of the reference (include/annsearch.h:58-83).  The
-  // counters exist so drivers that print them compile; the GPU path does not
-  // update them.
+  // Public members of the reference (include/annsearch.h:58-83); drivers
+  // read and reset the counters directly.
   std::atomic<int> hop_count{0};
   float ub_ratio = 0;
   int64_t dist_comps = 0;

@@ -63,6 +63,9 @@ SIGNATURES = {
     "ss_set_stage_layout": (_i32, [_vp, _i32, _i32]),
     "ss_search_scatter_batch": (_i32, [_vp, _f32p, _u32, _i32, _i32, _i32, _i32, ctypes.c_uint64,
                                        _u32p, _f32p]),
+    "ss_search_scatter_batch_stats": (_i32, [_vp, _f32p, _u32, _i32, _i32, _i32, _i32,
+                                             ctypes.c_uint64, _u32p, _f32p, _u32p, _u32p, _u32p,
+                                             _u32p]),
     "ss_search_scatter_batch_device": (_i32, [_vp, _vp, _u32, _i32, _i32, _i32, _i32,
                                               ctypes.c_uint64, _vp, _vp, _vp, _vp, _vp]),
     "ss_bruteforce": (_i32, [_vp, _f32p, _u32, _i32, _u32p, _f32p]),

@@ -262,6 +262,24 @@ class ANNSearch:
             int(bool(early_termination)), int(seed), _ptr(ids, _u32p), _ptr(dists, _f32p)))
         return ids, dists
 
+    def search_scatter_stats(self, queries, K: int, L: int, num_threads: int,
+                             early_termination: bool = False, seed: int = 1):
+        """``search_scatter`` plus the reference engine's per-query counters:
+        returns (ids, dists, counters) with counters a dict of nq-long uint32
+        arrays: ``ndc_sum`` (dist_comps), ``ndc_max`` / ``ndc_min`` (one warp's
+        most / fewest evaluations) and ``hops_sum`` (expansions)."""
+        q = _f32(queries).reshape(-1, self.dimension)
+        nq = q.shape[0]
+        ids = np.empty((nq, K), dtype=np.uint32)
+        dists = np.empty((nq, K), dtype=np.float32)
+        cnt = {k: np.empty(nq, dtype=np.uint32) for k in ("ndc_sum", "ndc_max", "ndc_min",
+                                                         "hops_sum")}
+        self._check(self._lib.ss_search_scatter_batch_stats(
+            self._h, _ptr(q, _f32p), nq, int(K), int(L), int(num_threads),
+            int(bool(early_termination)), int(seed), _ptr(ids, _u32p), _ptr(dists, _f32p),
+            *(_ptr(cnt[k], _u32p) for k in ("ndc_sum", "ndc_max", "ndc_min", "hops_sum"))))
+        return ids, dists, cnt
+
     def search_scatter_device(self, queries, nq: int, K: int, L: int, num_threads: int, ids,
                               dists=None, early_termination: bool = False, seed: int = 1,
                               ndc=None, hops=None, stream=None):

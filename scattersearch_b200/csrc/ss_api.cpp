@@ -15,6 +15,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "scattersearch.h"
@@ -415,7 +416,8 @@ int launch_intra(ss_index *h, SearchCtx *c, const float *d_q, uint32_t nq, int K
 
 int launch_scatter(ss_index *h, SearchCtx *c, const float *d_q, uint32_t nq, int K, int L, int W,
                    int et, uint64_t seed, uint32_t *d_ids, float *d_dists, uint32_t *d_ndc,
-                   uint32_t *d_hops, cudaStream_t stream) {
+                   uint32_t *d_hops, cudaStream_t stream, uint32_t *d_ndc_max = nullptr,
+                   uint32_t *d_ndc_min = nullptr) {
   ssb::GraphView g = h->view();
   ssb::SmemPlan plan = ssb::plan_scatter_smem(g, L, W);
   if (ssb::scatter_smem_bytes(plan, W) > 227 * 1024)
@@ -434,6 +436,8 @@ int launch_scatter(ss_index *h, SearchCtx *c, const float *d_q, uint32_t nq, int
   a.dists = d_dists;
   a.ndc = d_ndc;
   a.hops = d_hops;
+  a.ndc_max = d_ndc_max;
+  a.ndc_min = d_ndc_min;
   a.status = c->status.as<int32_t>();
   a.spill_bits = c->spill.as<uint32_t>();
   a.spill_words = spill_words(h);
@@ -1077,6 +1081,14 @@ int ss_bruteforce_device(ss_index *h, const float *queries, uint32_t nq, int k, 
 int ss_search_scatter_batch(ss_index *h, const float *queries, uint32_t nq, int K, int L,
                             int num_threads, int early_termination, uint64_t seed, uint32_t *ids,
                             float *dists) {
+  return ss_search_scatter_batch_stats(h, queries, nq, K, L, num_threads, early_termination, seed,
+                                       ids, dists, nullptr, nullptr, nullptr, nullptr);
+}
+
+int ss_search_scatter_batch_stats(ss_index *h, const float *queries, uint32_t nq, int K, int L,
+                                  int num_threads, int early_termination, uint64_t seed,
+                                  uint32_t *ids, float *dists, uint32_t *ndc_sum,
+                                  uint32_t *ndc_max, uint32_t *ndc_min, uint32_t *hops_sum) {
   int rc = check_scatter_args(h, K, L, num_threads);
   if (rc) return rc;
   if (nq == 0) return SS_OK;
@@ -1086,14 +1098,23 @@ int ss_search_scatter_batch(ss_index *h, const float *queries, uint32_t nq, int 
   SearchCtx *c = lease.c;
   if (!c) return set_err(h, SS_ERR_CUDA, "cannot create a stream");
   const size_t total = (size_t)nq * K;
+  const bool stats = ndc_sum || ndc_max || ndc_min || hops_sum;
   SS_CUDA(h, c->q.ensure((size_t)nq * h->dim * 4), "query buffer");
   SS_CUDA(h, c->ids.ensure(total * 4), "ids buffer");
   SS_CUDA(h, c->dists.ensure(total * 4), "dists buffer");
+  if (stats) {  // four counters per query: sum, max, min of evaluations, hops
+    SS_CUDA(h, c->ndc.ensure((size_t)nq * 3 * 4), "counter buffer");
+    SS_CUDA(h, c->hops.ensure((size_t)nq * 4), "counter buffer");
+  }
+  uint32_t *d_sum = stats ? c->ndc.as<uint32_t>() : nullptr;
+  uint32_t *d_max = stats ? d_sum + nq : nullptr, *d_min = stats ? d_sum + 2 * (size_t)nq : nullptr;
+  uint32_t *d_hops = stats ? c->hops.as<uint32_t>() : nullptr;
   SS_CUDA(h, cudaMemcpyAsync(c->q.p, queries, (size_t)nq * h->dim * 4, cudaMemcpyHostToDevice,
                              c->stream),
           "query upload");
   rc = launch_scatter(h, c, c->q.as<float>(), nq, K, L, num_threads, early_termination, seed,
-                      c->ids.as<uint32_t>(), c->dists.as<float>(), nullptr, nullptr, c->stream);
+                      c->ids.as<uint32_t>(), c->dists.as<float>(), d_sum, d_hops, c->stream,
+                      d_max, d_min);
   if (rc) return rc;
   c->h_status.resize(nq);
   SS_CUDA(h, cudaMemcpyAsync(ids, c->ids.p, total * 4, cudaMemcpyDeviceToHost, c->stream),
@@ -1101,6 +1122,13 @@ int ss_search_scatter_batch(ss_index *h, const float *queries, uint32_t nq, int 
   if (dists)
     SS_CUDA(h, cudaMemcpyAsync(dists, c->dists.p, total * 4, cudaMemcpyDeviceToHost, c->stream),
             "dists download");
+  const std::pair<uint32_t *, const uint32_t *> outs[4] = {
+      {ndc_sum, d_sum}, {ndc_max, d_max}, {ndc_min, d_min}, {hops_sum, d_hops}};
+  for (const auto &o : outs)
+    if (o.first)
+      SS_CUDA(h, cudaMemcpyAsync(o.first, o.second, (size_t)nq * 4, cudaMemcpyDeviceToHost,
+                                 c->stream),
+              "counter download");
   SS_CUDA(h, cudaMemcpyAsync(c->h_status.data(), c->status.p, (size_t)nq * 4,
                              cudaMemcpyDeviceToHost, c->stream),
           "status download");

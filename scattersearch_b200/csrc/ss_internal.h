@@ -32,6 +32,8 @@ struct BatchArgs {
   uint32_t *ids;
   float *dists;          // may be null
   uint32_t *ndc, *hops;  // may be null
+  uint32_t *ndc_max, *ndc_min;  // scatter kernel: per query, one warp's most / fewest
+                                // distance evaluations (may be null)
   int32_t *status;       // nq entries, may be null
   uint32_t *work_counter;  // persistent work queue head; null = static schedule
   uint32_t *spill_bits;    // per-slot visited bitsets, spill_words each

@@ -1465,6 +1465,7 @@ struct ScatterCtl {
   int vis_spilled;          // hash full: new ids go to the global bitset
   int status;
   unsigned ndc, hops;
+  unsigned ndc_max, ndc_min;      // one warp's most / fewest distance evaluations
   int good[kMaxScatter];          // 1: pool head better than the winning vote
   int reached[kMaxScatter];       // voted
   unsigned version[kMaxScatter];  // pool sequence counters (odd while changing)
@@ -1604,6 +1605,8 @@ __global__ void __launch_bounds__(512) scatter_search_kernel(GraphView g, BatchA
     ctl->status = kStatusOk;
     ctl->ndc = 0;
     ctl->hops = 0;
+    ctl->ndc_max = 0;
+    ctl->ndc_min = 0xFFFFFFFFu;
   }
   if (threadIdx.x < kMaxScatter) {
     ctl->good[threadIdx.x] = 0;
@@ -1828,6 +1831,8 @@ __global__ void __launch_bounds__(512) scatter_search_kernel(GraphView g, BatchA
   if (lane == 0) {
     atomicAdd(&ctl->ndc, ndc);
     atomicAdd(&ctl->hops, hops);
+    atomicMax(&ctl->ndc_max, ndc);
+    atomicMin(&ctl->ndc_min, ndc);
     if (status != kStatusOk) atomicExch(&ctl->status, status);
   }
   __syncthreads();
@@ -1876,6 +1881,8 @@ __global__ void __launch_bounds__(512) scatter_search_kernel(GraphView g, BatchA
   if (threadIdx.x == 0) {
     if (a.ndc) a.ndc[q_idx] = ctl->ndc;
     if (a.hops) a.hops[q_idx] = ctl->hops;
+    if (a.ndc_max) a.ndc_max[q_idx] = ctl->ndc_max;
+    if (a.ndc_min) a.ndc_min[q_idx] = ctl->ndc_min;
     if (a.status) a.status[q_idx] = ctl->status;
   }
 }
