@@ -691,6 +691,14 @@ __device__ __forceinline__ int accept_candidates(const WarpSmem &s, int nc, int 
         }
       }
     }
+    if (check_dups) {
+      // copies of one id in this 32-candidate chunk (the fresh ids of a row's
+      // chunks are compacted, so they need not sit in different chunks
+      // here): the first in adjacency order stays
+      const unsigned am0 = __ballot_sync(kFull, acc);
+      const unsigned same = __match_any_sync(kFull, acc ? id : kNoneId);
+      if (acc && (same & am0 & lanemask_lt)) acc = false;
+    }
     const unsigned am = __ballot_sync(kFull, acc);
     if (acc) {
       const int pos = na + __popc(am & lanemask_lt);
@@ -1446,14 +1454,18 @@ __global__ void __launch_bounds__(512) intra_search_kernel(GraphView g, BatchArg
 //          padded to L with random unvisited ids (:552-575);
 //   ET     the pool starts with the neighbours only; at the warp's 50th
 //          expansion it votes with its K-th distance; once all have voted,
-//          warps whose best entry is worse than the winning vote stop and
-//          (like the others that finish early) continue from unexplored
-//          entries copied out of a "good" warp's pool; the winner finishing
-//          stops every warp (:858-999, :1368-1455).
+//          warps whose best entry is worse than the winning vote stop.
+//          Those, like the others that finish early, steal every unexplored
+//          entry of one "good" warp's pool (marking them explored there, so
+//          that warp, the winner included, has less left to do), peek at a
+//          few entries of a second good warp, and continue from their own
+//          pool; the winner finishing stops every warp (:858-999,
+//          :1368-1455).
 // Entry points and pads come from a counter-based hash of (seed, query, warp)
-// instead of rand(); the election's ties go to the lower warp; and copies out
-// of another warp's pool are taken under that pool's sequence counter, where
-// the reference reads them unsynchronised.
+// instead of rand(); the election's ties go to the lower warp; entries are
+// read out of another warp's pool under that pool's sequence counter, and a
+// stolen entry is marked explored by compare-and-swap on its id, where the
+// reference reads and writes the other thread's pool unsynchronised.
 constexpr int kMaxScatter = SS_SCATTER_MAX_WARPS;
 constexpr int kElectionHop = 50;
 
@@ -1516,40 +1528,48 @@ __device__ __forceinline__ void scatter_reserve(Visited &v, ScatterCtl *ctl, int
   }
 }
 
-// Copies up to `cap` unexplored entries of warp t's pool, taken from its end
-// (as SearchUntilBestThreadStop does), into this warp's cid/ckey; returns how
-// many, or 0 when the pool changed under every attempt.
-__device__ __forceinline__ int scatter_copy_unexplored(const WarpSmem &src, ScatterCtl *ctl, int t,
-                                                       const WarpSmem &dst, int cap, int lane) {
+// Takes unexplored entries of warp t's pool in slots [b-31, b] (b counts down
+// from the pool's end; slot 0 is never taken), as SearchUntilBestThreadStop
+// walks a good thread's pool from its end (annsearch.cpp:1384-1396 steals,
+// :1402-1413 peeks), into this warp's cid/ckey.  The window is read under
+// t's sequence counter (a consistent copy, up to 4 attempts).  At most
+// `limit` entries are taken, the ones nearest the pool's end first.  With
+// `mark` (a steal) each is then marked explored in t's pool by a
+// compare-and-swap on its id, and only the entries this warp marked are kept:
+// one that t moved meanwhile stays t's to expand.  Returns how many entries
+// went to cid/ckey (0 also when every attempt saw the pool change).
+__device__ __forceinline__ int scatter_take_window(const WarpSmem &src, ScatterCtl *ctl, int t,
+                                                   const WarpSmem &dst, int b, bool mark, int limit,
+                                                   int lane) {
   const unsigned lanemask_lt = (1u << lane) - 1u;
-  for (int attempt = 0; attempt < 4; ++attempt) {
+  const int j = b - lane;
+  uint32_t id = 0, key = 0;
+  bool un = false, valid = false;
+  for (int attempt = 0; attempt < 4 && !valid; ++attempt) {
     const unsigned v0 = uniform_load(&ctl->version[t], lane);
     if (v0 & 1u) continue;
     __threadfence_block();
-    const int sz = uniform_load(&ctl->size[t], lane);
-    int got = 0;
-    for (int b = sz - 1; b >= 1 && got < cap; b -= 32) {
-      const int j = b - lane;
-      uint32_t id = 0, key = 0;
-      bool un = false;
-      if (j >= 1) {
-        id = *(volatile uint32_t *)&src.pid[j];
-        key = *(volatile uint32_t *)&src.pk[j];
-        un = !(id & kExplored);
-      }
-      const unsigned m = __ballot_sync(kFull, un);
-      const int pos = got + __popc(m & lanemask_lt);
-      if (un && pos < cap) {
-        dst.cid[pos] = id;
-        dst.ckey[pos] = key;
-      }
-      got = min(cap, got + __popc(m));
+    un = false;
+    if (j >= 1) {
+      id = *(volatile uint32_t *)&src.pid[j];
+      key = *(volatile uint32_t *)&src.pk[j];
+      un = !(id & kExplored);
     }
     __threadfence_block();
-    const unsigned v1 = uniform_load(&ctl->version[t], lane);
-    if (v0 == v1) return got;
+    valid = uniform_load(&ctl->version[t], lane) == v0;
   }
-  return 0;
+  if (!valid) return 0;
+  const unsigned um = __ballot_sync(kFull, un);
+  bool take = un && __popc(um & lanemask_lt) < limit;
+  if (mark && take) take = atomicCAS(&src.pid[j], id, id | kExplored) == id;
+  const unsigned tm = __ballot_sync(kFull, take);
+  if (take) {
+    const int pos = __popc(tm & lanemask_lt);
+    dst.cid[pos] = id;
+    dst.ckey[pos] = key;
+  }
+  __syncwarp();
+  return __popc(tm);
 }
 
 template <int NB, int RCH, int PITEMS>
@@ -1699,26 +1719,43 @@ __global__ void __launch_bounds__(512) scatter_search_kernel(GraphView g, BatchA
   const bool is_et = et != 0;
   for (int phase = 0; phase < 2 && status == kStatusOk; ++phase) {
     if (phase == 1) {
-      // ET: a warp that is not the winner continues from unexplored entries
-      // of good warps while the winner runs (SearchUntilBestThreadStop)
+      // ET: a warp that is not the winner continues while the winner runs
+      // (SearchUntilBestThreadStop, annsearch.cpp:1368-1455): it steals
+      // every unexplored entry of one good warp (up to 10 random draws),
+      // marking them explored there, then peeks at a few of a second random
+      // good warp, and goes on from its own pool.
       if (!is_et || uniform_load(&ctl->finish, lane)) break;
       const unsigned long long best = uniform_load(&ctl->best, lane);
       if (best != ~0ull && (int)(best & 0xFFFFFFFFu) == warp) break;
+      need_identify = false;  // the stealing loop has no election (:1417-1454)
+      dup_check = true;
       int target = -1;
       for (int round = 0; round < 10 && target < 0; ++round) {
+        if (uniform_load(&ctl->finish, lane)) break;
         const int t = (int)(scatter_rng(seed, q_idx, warp, 100000u + round) % (uint32_t)W);
         if (t != warp && uniform_load(&ctl->reached[t], lane) && uniform_load(&ctl->good[t], lane))
           target = t;
       }
-      if (target < 0) break;
-      dup_check = true;
-      const WarpSmem src = carve(target);
-      const int got = scatter_copy_unexplored(src, ctl, target, s, (int)p.cand_cap, lane);
-      if (got > 0 && size > 0) {
-        __syncwarp();
-        const uint32_t thr = s.pk[size - 1];
-        const int na = accept_candidates<RCH>(s, got, size, thr, true, lane);
-        if (na > 0) {
+      const int peek = (int)(scatter_rng(seed, q_idx, warp, 100010u) % (uint32_t)W);
+      int taken = 0;
+      for (int round = 0; round < 2; ++round) {
+        const int t = round == 0 ? target : peek;
+        if (t < 0 || t == warp) continue;
+        if (round == 1 && !(uniform_load(&ctl->reached[t], lane) && uniform_load(&ctl->good[t], lane)))
+          continue;
+        const WarpSmem src = carve(t);
+        const int tsize = uniform_load(&ctl->size[t], lane);
+        // a steal takes all; the peek takes entries until 21 were taken in
+        // both rounds together, at least one (:1402-1412)
+        int left = round == 0 ? L : max(1, 21 - taken);
+        for (int b = tsize - 1; b >= 1 && left > 0 && size > 0; b -= 32) {
+          const int got = scatter_take_window(src, ctl, t, s, b, round == 0, left, lane);
+          taken += got;
+          left -= got;
+          if (got == 0) continue;
+          const uint32_t thr = s.pk[size - 1];
+          const int na = accept_candidates<RCH>(s, got, size, thr, true, lane);
+          if (na == 0) continue;
           __syncwarp();
           uint32_t nkey[RCH], nid[RCH];
           int npos[RCH];
