@@ -177,17 +177,33 @@ __device__ __forceinline__ void qh_keys(const QHash &h, uint32_t id, uint32_t &b
   t2 = (f2 & h.rmask) | 0x8000u;
 }
 
-__device__ __forceinline__ bool bucket_has(uint4 v, uint32_t t) {
-  const uint32_t tt = t | (t << 16);
-  return (__vcmpeq2(v.x, tt) | __vcmpeq2(v.y, tt) | __vcmpeq2(v.z, tt) | __vcmpeq2(v.w, tt)) != 0u;
+// Nonzero iff one of the two 16-bit halves of x is zero: x - 1 per half sets
+// bit 15 of a half and leaves it clear in ~x only when that half is zero,
+// and a borrow into the upper half only comes from a zero lower half.
+__device__ __forceinline__ uint32_t has_zero_half(uint32_t x) {
+  return (x - 0x00010001u) & ~x & 0x80008000u;
 }
 
-// 8-bit mask of empty slots (slot s = 16-bit half s of the bucket).
+__device__ __forceinline__ bool bucket_has(uint4 v, uint32_t t) {
+  const uint32_t tt = t | (t << 16);
+  return (has_zero_half(v.x ^ tt) | has_zero_half(v.y ^ tt) | has_zero_half(v.z ^ tt) |
+          has_zero_half(v.w ^ tt)) != 0u;
+}
+
+// 8-bit mask of the empty slots of a bucket: bit p stands for slot p ^ 6
+// (slot s = 16-bit half s of the bucket).  A tag holds at most 14 remainder
+// bits and the choice flag in bit 15, so bit 14 is set only in the empty
+// marker 0xFFFF; the four words' bit-14/30 flags are shifted into one byte.
 __device__ __forceinline__ uint32_t bucket_empty(uint4 v) {
-  const uint32_t e0 = __vcmpeq2(v.x, 0xFFFFFFFFu), e1 = __vcmpeq2(v.y, 0xFFFFFFFFu);
-  const uint32_t e2 = __vcmpeq2(v.z, 0xFFFFFFFFu), e3 = __vcmpeq2(v.w, 0xFFFFFFFFu);
-  return (e0 & 1u) | ((e0 >> 15) & 2u) | ((e1 & 1u) << 2) | ((e1 >> 13) & 8u) |
-         ((e2 & 1u) << 4) | ((e2 >> 11) & 32u) | ((e3 & 1u) << 6) | ((e3 >> 9) & 128u);
+  const uint32_t m = (v.x & 0x40004000u) | ((v.y & 0x40004000u) >> 2) |
+                     ((v.z & 0x40004000u) >> 4) | ((v.w & 0x40004000u) >> 6);
+  return ((m >> 8) & 0x55u) | ((m >> 23) & 0xAAu);
+}
+
+// Slot of the (r+1)-th empty slot in an empty mask from bucket_empty.
+__device__ __forceinline__ uint32_t nth_empty_slot(uint32_t e, int r) {
+  for (int i = 0; i < r; ++i) e &= e - 1u;
+  return (uint32_t)(__ffs(e) - 1) ^ 6u;
 }
 
 // 16-byte shared-memory load that is never cached in registers or reordered
@@ -235,7 +251,7 @@ __device__ __forceinline__ void qh_record(QHash &h, const QProbe &pr, uint32_t i
   if (ins) {
     uint32_t sl;
     if (r < __popc(e)) {
-      sl = __fns(e, 0, r + 1);
+      sl = nth_empty_slot(e, r);
     } else {
       sl = (id * kMix3) >> 29;
       ev = true;
