@@ -505,9 +505,21 @@ def measure_online(idx, wl, rates=(1_000, 10_000, 50_000, 100_000, 200_000),
             log(f"online {rate}/s: sustained {row['sustained_qps']:.0f}/s p50 {row['p50_ms']:.2f} "
                 f"p99 {row['p99_ms']:.2f} p999 {row['p999_ms']:.2f} ms recall {row['recall@10']:.4f}")
     return {"K": "10 or 100 per request", "L": "uniform in [64, 400] per request",
-            "max_batch": 256, "slots": 4, "arrivals": "Poisson",
+            "max_batch": 256, "slots": 4, "arrivals": "Poisson", "host_cpu": host_cpu(),
             "window": f"max({seconds:g} s, 2000 requests) per rate, at most {max_requests}",
             "latency": "scheduled arrival to result on the host", "rates": out}
+
+
+def host_cpu():
+    """Host cores this process may use and the container's CPU bandwidth limit
+    (cgroup v2 cpu.max: quota and period in microseconds, or "max")."""
+    out = {"affinity": cpu_threads()}
+    try:
+        with open("/sys/fs/cgroup/cpu.max") as f:
+            out["cgroup_cpu_max"] = f.read().strip()
+    except OSError:
+        out["cgroup_cpu_max"] = None
+    return out
 
 
 def parity_record(wl, ids_np, L):

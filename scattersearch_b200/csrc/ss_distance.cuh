@@ -46,55 +46,26 @@ __device__ __forceinline__ int block_at(int t, int nb) {
   return (nb & 1) ? (t == 0 ? nb - 1 : t - 1) : t;
 }
 
-// Two floats in one 64-bit register (first in the low half) and sm_100's
-// paired FP32 arithmetic on them: each half is a separate IEEE operation with
-// round-to-nearest-even, exactly the scalar add.rn / sub.rn / mul.rn, so
-// results are bit-identical to the scalar form while one instruction does
-// two lanes' work.  Subnormals are kept (no .ftz), as in the scalar form.
-__device__ __forceinline__ uint64_t f2_pack(float lo, float hi) {
-  uint64_t r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-  return r;
-}
-__device__ __forceinline__ void f2_unpack(uint64_t v, float &lo, float &hi) {
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
-}
-__device__ __forceinline__ uint64_t f2_sub(uint64_t a, uint64_t b) {
-  uint64_t r;
-  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-  return r;
-}
-__device__ __forceinline__ uint64_t f2_mul(uint64_t a, uint64_t b) {
-  uint64_t r;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-  return r;
-}
-__device__ __forceinline__ uint64_t f2_add(uint64_t a, uint64_t b) {
-  uint64_t r;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-  return r;
-}
-
 // One 8-float block's contribution to four of the eight lane partials
 // (reference lanes 4h..4h+3 of distance.cpp:47-51): a_j += (q_j - v_j)^2
 // (L2) or a_j += q_j * v_j (inner product), each operation rounded once.
+// Scalar instructions on purpose: the paired FP32 forms (sub/mul/add.rn.f32x2)
+// were measured on this GPU to return distances that differ from these in
+// the last bit, which would break bit-exact parity with the reference.
 __device__ __forceinline__ void acc_l2(float &a0, float &a1, float &a2, float &a3, float4 q,
                                        float4 v) {
-  uint64_t lo = f2_pack(a0, a1), hi = f2_pack(a2, a3);
-  const uint64_t d0 = f2_sub(f2_pack(q.x, q.y), f2_pack(v.x, v.y));
-  const uint64_t d1 = f2_sub(f2_pack(q.z, q.w), f2_pack(v.z, v.w));
-  lo = f2_add(lo, f2_mul(d0, d0));
-  hi = f2_add(hi, f2_mul(d1, d1));
-  f2_unpack(lo, a0, a1);
-  f2_unpack(hi, a2, a3);
+  float d;
+  d = __fsub_rn(q.x, v.x); a0 = __fadd_rn(a0, __fmul_rn(d, d));
+  d = __fsub_rn(q.y, v.y); a1 = __fadd_rn(a1, __fmul_rn(d, d));
+  d = __fsub_rn(q.z, v.z); a2 = __fadd_rn(a2, __fmul_rn(d, d));
+  d = __fsub_rn(q.w, v.w); a3 = __fadd_rn(a3, __fmul_rn(d, d));
 }
 __device__ __forceinline__ void acc_ip(float &a0, float &a1, float &a2, float &a3, float4 q,
                                        float4 v) {
-  uint64_t lo = f2_pack(a0, a1), hi = f2_pack(a2, a3);
-  lo = f2_add(lo, f2_mul(f2_pack(q.x, q.y), f2_pack(v.x, v.y)));
-  hi = f2_add(hi, f2_mul(f2_pack(q.z, q.w), f2_pack(v.z, v.w)));
-  f2_unpack(lo, a0, a1);
-  f2_unpack(hi, a2, a3);
+  a0 = __fadd_rn(a0, __fmul_rn(q.x, v.x));
+  a1 = __fadd_rn(a1, __fmul_rn(q.y, v.y));
+  a2 = __fadd_rn(a2, __fmul_rn(q.z, v.z));
+  a3 = __fadd_rn(a3, __fmul_rn(q.w, v.w));
 }
 
 // Distance between the shared-memory query and base row `id`, computed by a

@@ -1827,7 +1827,12 @@ __global__ void __launch_bounds__(512) scatter_search_kernel(GraphView g, BatchA
         status = kStatusHopLimit;
         break;
       }
-      const uint32_t node = s.pid[k];
+      // A stealing warp may mark slot k explored after the ballot above (the
+      // entry is then its to expand), so the slot is read once, by lane 0,
+      // and skipped when taken; the node id never carries the explored bit.
+      const uint32_t raw = uniform_load(&s.pid[k], lane);
+      if (raw & kExplored) continue;
+      const uint32_t node = raw;
       const uint32_t thr = s.pk[size - 1];
       __syncwarp();
       if (lane == 0) s.pid[k] = node | kExplored;

@@ -419,34 +419,41 @@ int ss_server_replay(ss_server *s, const float *queries, uint32_t nq, const int3
   std::vector<int64_t> off(nq, 0);
   for (uint32_t i = 1; i < nq; ++i) off[i] = off[i - 1] + Ks[i - 1];
   std::atomic<int> gen_rc{SS_OK};
-  std::atomic<uint32_t> submitted{0};
+  // The generator sleeps until each arrival time and then submits every
+  // request that is due (it never spins: a busy client thread competes with
+  // the dispatcher for the host's cores); latency still runs from the
+  // scheduled arrival, so a late wake-up counts against the server.
+  std::mutex sub_mu;
+  std::condition_variable sub_cv;
+  uint32_t submitted = 0;
   const Clock::time_point t0 = Clock::now();
   std::thread gen([&] {
     for (uint32_t i = 0; i < nq; ++i) {
       const auto t_arr = t0 + std::chrono::duration_cast<Clock::duration>(
                                   std::chrono::duration<double, std::micro>(arrival_us[i]));
-      while (Clock::now() < t_arr) {
-        const auto left = t_arr - Clock::now();
-        if (left > std::chrono::microseconds(200)) std::this_thread::sleep_for(left / 2);
-      }
+      if (Clock::now() < t_arr) std::this_thread::sleep_until(t_arr);
       int rc;
       for (;;) {
         rc = s->submit_at(queries + (size_t)i * s->dim, Ks[i], Ls[i], t_arr, &tickets[i]);
         if (rc != SS_ERR_BUSY) break;
         std::this_thread::sleep_for(std::chrono::microseconds(50));
       }
-      if (rc != SS_OK) {
-        gen_rc.store(rc);
-        break;
+      if (rc != SS_OK) gen_rc.store(rc);
+      {
+        std::lock_guard<std::mutex> lk(sub_mu);
+        submitted = rc == SS_OK ? i + 1 : nq + 1;  // nq + 1: stopped early
       }
-      submitted.store(i + 1, std::memory_order_release);
+      sub_cv.notify_one();
+      if (rc != SS_OK) break;
     }
   });
   int rc = SS_OK;
   for (uint32_t i = 0; i < nq; ++i) {
-    while (submitted.load(std::memory_order_acquire) <= i && gen_rc.load() == SS_OK)
-      std::this_thread::sleep_for(std::chrono::microseconds(20));
-    if (submitted.load(std::memory_order_acquire) <= i) break;
+    {
+      std::unique_lock<std::mutex> lk(sub_mu);
+      sub_cv.wait(lk, [&] { return submitted > i; });
+      if (submitted == nq + 1 && tickets[i] == 0) break;
+    }
     double lat = 0.0;
     const int w = ss_server_wait(s, tickets[i], -1, ids + off[i], dists ? dists + off[i] : nullptr,
                                  &lat);
