@@ -478,7 +478,7 @@ def measure_online(idx, wl, rates=(1_000, 10_000, 50_000, 100_000, 200_000),
     nq = min(len(Q), len(gt))
     rng = np.random.default_rng(seed)
     out = []
-    with Server(idx, max_batch=256, max_inflight=4, K_max=100, L_max=400) as srv:
+    with Server(idx, max_batch=256, max_inflight=8, K_max=100, L_max=400) as srv:
         warm = min(nq, 4096)
         srv.replay(Q[:warm], np.full(warm, 100, np.int32), np.full(warm, 400, np.int32),
                    poisson_arrivals(warm, 100_000, seed=1))
@@ -488,14 +488,15 @@ def measure_online(idx, wl, rates=(1_000, 10_000, 50_000, 100_000, 200_000),
             sel = np.arange(n) % nq
             Ks = rng.choice(np.array([10, 100], np.int32), n)
             Ls = np.maximum(Ks, rng.integers(64, 401, n)).astype(np.int32)
+            arr = poisson_arrivals(n, rate, seed=rate)
             t0 = time.perf_counter()
-            ids, _, off, lat = srv.replay(Q[sel], Ks, Ls, poisson_arrivals(n, rate, seed=rate))
+            ids, _, off, lat = srv.replay(Q[sel], Ks, Ls, arr)
             wall = time.perf_counter() - t0
             st = srv.stats(reset=True)
             first10 = ids[off[:, None] + np.arange(10)[None, :]]
             row = {"offered_qps": rate if rate != saturation else None,
                    "saturating_burst": rate == saturation, "requests": n,
-                   "sustained_qps": n / wall,
+                   "arrival_qps": n / max(1e-9, arr[-1] / 1e6), "sustained_qps": n / wall,
                    "p50_ms": float(np.percentile(lat, 50)) / 1e3,
                    "p99_ms": float(np.percentile(lat, 99)) / 1e3,
                    "p999_ms": float(np.percentile(lat, 99.9)) / 1e3,
@@ -505,7 +506,7 @@ def measure_online(idx, wl, rates=(1_000, 10_000, 50_000, 100_000, 200_000),
             log(f"online {rate}/s: sustained {row['sustained_qps']:.0f}/s p50 {row['p50_ms']:.2f} "
                 f"p99 {row['p99_ms']:.2f} p999 {row['p999_ms']:.2f} ms recall {row['recall@10']:.4f}")
     return {"K": "10 or 100 per request", "L": "uniform in [64, 400] per request",
-            "max_batch": 256, "slots": 4, "arrivals": "Poisson", "host_cpu": host_cpu(),
+            "max_batch": 256, "slots": 8, "arrivals": "Poisson", "host_cpu": host_cpu(),
             "window": f"max({seconds:g} s, 2000 requests) per rate, at most {max_requests}",
             "latency": "scheduled arrival to result on the host", "rates": out}
 

@@ -67,6 +67,11 @@ def _lib_oracle() -> ctypes.CDLL:
         lib.sso_bruteforce_f64.argtypes = [
             _c_f32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, _c_f32p, ctypes.c_uint32,
             ctypes.c_int, _c_u32p, _c_f64p, ctypes.c_int]
+        lib.sso_scatter_plain.restype = ctypes.c_int
+        lib.sso_scatter_plain.argtypes = [
+            _c_f32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, _c_u32p, ctypes.c_uint32,
+            _c_f32p, ctypes.c_uint32, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint64,
+            _c_u32p, _c_u32p, ctypes.c_int]
         _libs["oracle"] = lib
     return _libs["oracle"]
 
@@ -178,6 +183,25 @@ def bruteforce_f64(base, queries, k: int, metric: int, nthreads: int | None = No
                                      _ptr(queries, _c_f32p), nq, k, _ptr(ids, _c_u32p),
                                      _ptr(dists, _c_f64p), nthreads or os.cpu_count() or 1)
     return ids, dists
+
+
+def scatter_plain(base, adj, metric: int, queries, K: int, L: int, T: int, seed: int = 1,
+                  nthreads: int | None = None):
+    """MultiThreadSearchArraySimulation's rules (T pools from random entry
+    points, padded to L, one shared visited set, K best of all pools) under
+    one fixed schedule: pools take one expansion each in turn, with an exact
+    visited set.  Returns (ids nq x K, distance evaluations per query)."""
+    base, adj, queries = _f32(base), _u32(adj), _f32(queries)
+    nq = queries.shape[0]
+    ids = np.zeros((nq, K), dtype=np.uint32)
+    ndc = np.zeros(nq, dtype=np.uint32)
+    rc = _lib_oracle().sso_scatter_plain(
+        _ptr(base, _c_f32p), base.shape[0], base.shape[1], metric, _ptr(adj, _c_u32p),
+        adj.shape[1], _ptr(queries, _c_f32p), nq, K, L, T, seed, _ptr(ids, _c_u32p),
+        _ptr(ndc, _c_u32p), nthreads or os.cpu_count() or 1)
+    if rc != 0:
+        raise ValueError("oracle scatter search rejected its arguments")
+    return ids, ndc
 
 
 def recall(ids, gt, k: int = 10) -> float:

@@ -293,3 +293,142 @@ int sso_bruteforce_f64(const float *base, uint32_t n, uint32_t dim, int metric,
   }
   return 0;
 }
+
+/* ---- ScatterSearch without election, restated for the recall check ------
+ * MultiThreadSearchArraySimulation (src/annsearch.cpp:532-699): T pools of
+ * L, each seeded with every neighbour of its own random entry point and
+ * padded to L with random unvisited ids (:552-575), all sharing one visited
+ * set; each pool runs the plain best-first rules; the answer is the K best
+ * of all pools, one copy per id (:646-668).  The reference's threads race on
+ * a shared bitset without atomics, so its result depends on their timing;
+ * this restatement fixes one schedule: the pools are set up in order and
+ * then take one expansion each in turn, with an exact visited set.  Entry
+ * points and pads come from a seeded counter hash.  ids: nq x K; ndc (may be
+ * NULL): distance evaluations per query, all pools together. */
+typedef struct { uint32_t id; float d; int explored; } sso_sent;
+
+static uint64_t sso_mix(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+static int sso_sent_cmp(const void *a, const void *b) {
+  const sso_sent *x = (const sso_sent *)a, *y = (const sso_sent *)b;
+  if (x->d < y->d) return -1;
+  if (x->d > y->d) return 1;
+  return x->id < y->id ? -1 : (x->id > y->id ? 1 : 0);
+}
+
+/* one expansion of pool p (size *sz, capacity L); returns 0 when nothing
+ * is left to expand */
+static int sso_scatter_hop(const float *base, uint32_t dim, int metric, const uint32_t *adj,
+                           uint32_t rstride, const float *q, sso_sent *p, int *sz, int L,
+                           unsigned char *vis, sso_sent *cand, sso_sent *tmp, uint32_t *ndc) {
+  int k = 0;
+  while (k < *sz && p[k].explored) ++k;
+  if (k >= *sz) return 0;
+  p[k].explored = 1;
+  const uint32_t *row = adj + (size_t)p[k].id * rstride;
+  const float thr = p[*sz - 1].d;
+  int nc = 0;
+  for (uint32_t m = 0; m < rstride && row[m] != SSO_NONE; ++m) {
+    const uint32_t id = row[m];
+    if (vis[id]) continue;
+    vis[id] = 1;
+    const float d = sso_distance(q, base + (size_t)id * dim, dim, metric);
+    ++*ndc;
+    if (d < thr) {
+      /* stable insertion by distance (adjacency order on ties) */
+      int j = nc++;
+      while (j > 0 && cand[j - 1].d > d) { cand[j] = cand[j - 1]; --j; }
+      cand[j].id = id; cand[j].d = d; cand[j].explored = 0;
+    }
+  }
+  /* merge, old entries first on equal distance, truncated to L */
+  int a = 0, o = 0, n = 0;
+  while (n < L && (o < *sz || a < nc)) {
+    if (a < nc && (o >= *sz || cand[a].d < p[o].d)) tmp[n++] = cand[a++];
+    else tmp[n++] = p[o++];
+  }
+  memcpy(p, tmp, sizeof(sso_sent) * (size_t)n);
+  *sz = n;
+  return 1;
+}
+
+int sso_scatter_plain(const float *base, uint32_t n, uint32_t dim, int metric,
+                      const uint32_t *adj, uint32_t rstride, const float *queries, uint32_t nq,
+                      int K, int L, int T, uint64_t seed, uint32_t *ids, uint32_t *ndc,
+                      int nthreads) {
+  if (K < 1 || L < K || T < 1 || n == 0) return -1;
+#pragma omp parallel num_threads(nthreads > 0 ? nthreads : 1)
+  {
+    unsigned char *vis = (unsigned char *)calloc(n, 1);
+    sso_sent *pools = (sso_sent *)malloc(sizeof(sso_sent) * (size_t)T * (size_t)L);
+    int *sz = (int *)malloc(sizeof(int) * (size_t)T);
+    int *live = (int *)malloc(sizeof(int) * (size_t)T);
+    sso_sent *cand = (sso_sent *)malloc(sizeof(sso_sent) * (size_t)(rstride + 1));
+    sso_sent *tmp = (sso_sent *)malloc(sizeof(sso_sent) * (size_t)(L + rstride + 1));
+    sso_sent *all = (sso_sent *)malloc(sizeof(sso_sent) * (size_t)T * (size_t)L);
+#pragma omp for schedule(dynamic, 1)
+    for (long qi = 0; qi < (long)nq; ++qi) {
+      const float *q = queries + (size_t)qi * dim;
+      uint32_t evals = 0;
+      uint64_t ctr = 0;
+      for (int t = 0; t < T; ++t) {
+        sso_sent *p = pools + (size_t)t * L;
+        const uint32_t ep = (uint32_t)(sso_mix(seed ^ ((uint64_t)qi << 32) ^ ((uint64_t)t << 20) ^ ctr++) % n);
+        int s = 0;
+        const uint32_t *row = adj + (size_t)ep * rstride;
+        for (uint32_t m = 0; m < rstride && row[m] != SSO_NONE && s < L; ++m) {
+          p[s++].id = row[m];
+          vis[row[m]] = 1;
+        }
+        while (s < L) {
+          uint32_t id = (uint32_t)(sso_mix(seed ^ ((uint64_t)qi << 32) ^ ((uint64_t)t << 20) ^ ctr++) % n);
+          uint32_t probes = 0;
+          while (vis[id] && probes++ < n) id = id + 1 == n ? 0 : id + 1;
+          if (vis[id]) break;
+          vis[id] = 1;
+          p[s++].id = id;
+        }
+        for (int j = 0; j < s; ++j) {
+          p[j].d = sso_distance(base + (size_t)p[j].id * dim, q, dim, metric);
+          p[j].explored = 0;
+        }
+        evals += (uint32_t)s;
+        /* stable sort by distance */
+        for (int j = 1; j < s; ++j) {
+          sso_sent x = p[j];
+          int i = j;
+          while (i > 0 && p[i - 1].d > x.d) { p[i] = p[i - 1]; --i; }
+          p[i] = x;
+        }
+        sz[t] = s;
+        live[t] = s > 0;
+      }
+      for (int any = 1; any;) {
+        any = 0;
+        for (int t = 0; t < T; ++t) {
+          if (!live[t]) continue;
+          live[t] = sso_scatter_hop(base, dim, metric, adj, rstride, q, pools + (size_t)t * L,
+                                    &sz[t], L, vis, cand, tmp, &evals);
+          any |= live[t];
+        }
+      }
+      int na = 0;
+      for (int t = 0; t < T; ++t)
+        for (int j = 0; j < sz[t]; ++j) all[na++] = pools[(size_t)t * L + j];
+      qsort(all, (size_t)na, sizeof(sso_sent), sso_sent_cmp);
+      int out = 0;
+      for (int j = 0; j < na && out < K; ++j)
+        if (j == 0 || all[j].id != all[j - 1].id) ids[(size_t)qi * K + out++] = all[j].id;
+      for (; out < K; ++out) ids[(size_t)qi * K + out] = SSO_NONE;
+      if (ndc) ndc[qi] = evals;
+      memset(vis, 0, n);  /* the next query starts unvisited */
+    }
+    free(vis); free(pools); free(sz); free(live); free(cand); free(tmp); free(all);
+  }
+  return 0;
+}

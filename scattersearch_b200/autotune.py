@@ -25,8 +25,9 @@ DEFAULT_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "scattersearch_b
 WPB_CANDIDATES = (1, 2, 4, 8)
 # (teams per CTA, shared row stages) layouts tried besides one stage per team
 SHARED_CANDIDATES = ((2, 1), (4, 2), (4, 3), (8, 3), (8, 4), (8, 5))
-# rows per row stage tried with one stage per team (16 = the default)
-STAGE_ROWS_CANDIDATES = (16, 12)
+# rows per row stage tried with one stage per team (16 = the default; 24 takes
+# most hops' fresh rows in one copy round trip, at fewer teams per SM)
+STAGE_ROWS_CANDIDATES = (16, 12, 24)
 _lock = threading.Lock()
 
 

@@ -1471,17 +1471,22 @@ __global__ void __launch_bounds__(512) intra_search_kernel(GraphView g, BatchArg
 //   ET     the pool starts with the neighbours only; at the warp's 50th
 //          expansion it votes with its K-th distance; once all have voted,
 //          warps whose best entry is worse than the winning vote stop.
-//          Those, like the others that finish early, steal every unexplored
-//          entry of one "good" warp's pool (marking them explored there, so
-//          that warp, the winner included, has less left to do), peek at a
-//          few entries of a second good warp, and continue from their own
-//          pool; the winner finishing stops every warp (:858-999,
-//          :1368-1455).
+//          Those, like the others that finish early, copy every unexplored
+//          entry of one "good" warp's pool, then a few entries of a second
+//          good warp, and continue from their own pool; the winner finishing
+//          stops every warp (:858-999, :1368-1455).
 // Entry points and pads come from a counter-based hash of (seed, query, warp)
-// instead of rand(); the election's ties go to the lower warp; entries are
-// read out of another warp's pool under that pool's sequence counter, and a
-// stolen entry is marked explored by compare-and-swap on its id, where the
-// reference reads and writes the other thread's pool unsynchronised.
+// instead of rand(); the election's ties go to the lower warp; and entries are
+// read out of another warp's pool under that pool's sequence counter, where
+// the reference reads the other thread's pool unsynchronised.
+// One rule is not carried over: the reference's thief also marks the stolen
+// entries explored in the good thread's pool (:1390).  On CPU threads that
+// is a race the owner mostly wins (it keeps expanding from the front of its
+// pool while the thief walks in from the end); on warps in lockstep the thief
+// marks the whole pool within one hop, the winner then has nothing left,
+// finishes and stops every warp, and recall fell below a single plain search
+// (0.947 against 0.982 on 50k x 96 unit vectors, L = 100, 4 warps).  Stolen
+// entries are therefore copied and left to their owner as well.
 constexpr int kMaxScatter = SS_SCATTER_MAX_WARPS;
 constexpr int kElectionHop = 50;
 
@@ -1544,19 +1549,16 @@ __device__ __forceinline__ void scatter_reserve(Visited &v, ScatterCtl *ctl, int
   }
 }
 
-// Takes unexplored entries of warp t's pool in slots [b-31, b] (b counts down
-// from the pool's end; slot 0 is never taken), as SearchUntilBestThreadStop
+// Copies unexplored entries of warp t's pool in slots [b-31, b] (b counts
+// down from the pool's end; slot 0 is never taken), as SearchUntilBestThreadStop
 // walks a good thread's pool from its end (annsearch.cpp:1384-1396 steals,
 // :1402-1413 peeks), into this warp's cid/ckey.  The window is read under
-// t's sequence counter (a consistent copy, up to 4 attempts).  At most
-// `limit` entries are taken, the ones nearest the pool's end first.  With
-// `mark` (a steal) each is then marked explored in t's pool by a
-// compare-and-swap on its id, and only the entries this warp marked are kept:
-// one that t moved meanwhile stays t's to expand.  Returns how many entries
-// went to cid/ckey (0 also when every attempt saw the pool change).
+// t's sequence counter (a consistent copy, up to 4 attempts); at most `limit`
+// entries are taken, the ones nearest the pool's end first.  The entries stay
+// unexplored in t's pool: see the kernel's comment on stealing.  Returns how
+// many went to cid/ckey (0 also when every attempt saw the pool change).
 __device__ __forceinline__ int scatter_take_window(const WarpSmem &src, ScatterCtl *ctl, int t,
-                                                   const WarpSmem &dst, int b, bool mark, int limit,
-                                                   int lane) {
+                                                   const WarpSmem &dst, int b, int limit, int lane) {
   const unsigned lanemask_lt = (1u << lane) - 1u;
   const int j = b - lane;
   uint32_t id = 0, key = 0;
@@ -1576,8 +1578,7 @@ __device__ __forceinline__ int scatter_take_window(const WarpSmem &src, ScatterC
   }
   if (!valid) return 0;
   const unsigned um = __ballot_sync(kFull, un);
-  bool take = un && __popc(um & lanemask_lt) < limit;
-  if (mark && take) take = atomicCAS(&src.pid[j], id, id | kExplored) == id;
+  const bool take = un && __popc(um & lanemask_lt) < limit;
   const unsigned tm = __ballot_sync(kFull, take);
   if (take) {
     const int pos = __popc(tm & lanemask_lt);
@@ -1736,10 +1737,9 @@ __global__ void __launch_bounds__(512) scatter_search_kernel(GraphView g, BatchA
   for (int phase = 0; phase < 2 && status == kStatusOk; ++phase) {
     if (phase == 1) {
       // ET: a warp that is not the winner continues while the winner runs
-      // (SearchUntilBestThreadStop, annsearch.cpp:1368-1455): it steals
-      // every unexplored entry of one good warp (up to 10 random draws),
-      // marking them explored there, then peeks at a few of a second random
-      // good warp, and goes on from its own pool.
+      // (SearchUntilBestThreadStop, annsearch.cpp:1368-1455): it copies every
+      // unexplored entry of one good warp (up to 10 random draws), then a few
+      // of a second random good warp, and goes on from its own pool.
       if (!is_et || uniform_load(&ctl->finish, lane)) break;
       const unsigned long long best = uniform_load(&ctl->best, lane);
       if (best != ~0ull && (int)(best & 0xFFFFFFFFu) == warp) break;
@@ -1761,11 +1761,11 @@ __global__ void __launch_bounds__(512) scatter_search_kernel(GraphView g, BatchA
           continue;
         const WarpSmem src = carve(t);
         const int tsize = uniform_load(&ctl->size[t], lane);
-        // a steal takes all; the peek takes entries until 21 were taken in
-        // both rounds together, at least one (:1402-1412)
+        // the first round takes all; the peek takes entries until 21 were
+        // taken in both rounds together, at least one (:1402-1412)
         int left = round == 0 ? L : max(1, 21 - taken);
         for (int b = tsize - 1; b >= 1 && left > 0 && size > 0; b -= 32) {
-          const int got = scatter_take_window(src, ctl, t, s, b, round == 0, left, lane);
+          const int got = scatter_take_window(src, ctl, t, s, b, left, lane);
           taken += got;
           left -= got;
           if (got == 0) continue;

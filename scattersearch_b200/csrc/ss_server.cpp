@@ -6,8 +6,9 @@
 // a few launch slots, each a CUDA stream with fixed device and pinned host
 // buffers for max_batch requests.  Whenever a slot is free and requests are
 // pending, it launches all of them (up to max_batch, each with its own K and
-// L) as one batched search on that slot's stream; a host callback marks the
-// slot done.  Requests arriving while launches run wait only for the next
+// L) as one batched search on that slot's stream, followed by an event that
+// the slot's completion thread waits for (blocking, woken by the driver)
+// before it marks the slot done.  Requests arriving while launches run wait only for the next
 // free slot, and launches on different slots overlap on the device (each
 // grid is sized to its own batch).  Every query's result is independent of
 // its batch: the kernel keeps no state shared between queries.
@@ -66,6 +67,13 @@ struct Slot {
   std::atomic<bool> done{false};
   Clock::time_point t_done;
   struct ss_server *owner = nullptr;
+  // completion: the event recorded after a batch's result copies, and the
+  // thread that blocks on it (armed by the dispatcher for each launch)
+  cudaEvent_t done_ev = nullptr;
+  std::thread waiter;
+  std::mutex wmu;
+  std::condition_variable wcv;
+  bool armed = false, quit = false;
 };
 
 template <class T>
@@ -118,18 +126,35 @@ struct ss_server {
   void finish_slot(Slot &sl);
   bool launch_slot(Slot &sl, std::unique_lock<std::mutex> &lk);
   int submit_at(const float *query, int K, int L, Clock::time_point t_arrival, uint64_t *ticket);
+  // Submits up to `count` requests at once (one lock, one wake-up); returns
+  // how many went in before the ring filled (or a negative error status).
+  int submit_many(const float *queries, const int32_t *Ks, const int32_t *Ls,
+                  const Clock::time_point *t_arrival, uint32_t count, uint64_t *tickets);
   void free_slots();
 };
 
 namespace {
 
-void CUDART_CB slot_done_cb(void *arg) {
-  Slot *sl = static_cast<Slot *>(arg);
-  sl->t_done = Clock::now();
-  sl->done.store(true, std::memory_order_release);
-  ss_server *s = sl->owner;
-  { std::lock_guard<std::mutex> lk(s->mu); }
-  s->cv_work.notify_all();
+// Completion thread of one launch slot: waits for each armed launch's event
+// (a blocking wait: the thread sleeps until the driver signals it), then
+// marks the slot done and wakes the dispatcher.  Each slot has its own
+// thread, so one late batch never holds up another slot's completion.
+void slot_waiter(Slot *sl, int device) {
+  cudaSetDevice(device);
+  for (;;) {
+    {
+      std::unique_lock<std::mutex> wl(sl->wmu);
+      sl->wcv.wait(wl, [sl] { return sl->armed || sl->quit; });
+      if (!sl->armed) return;  // quit with nothing in flight
+      sl->armed = false;
+    }
+    cudaEventSynchronize(sl->done_ev);
+    sl->t_done = Clock::now();
+    sl->done.store(true, std::memory_order_release);
+    ss_server *s = sl->owner;
+    { std::lock_guard<std::mutex> lk(s->mu); }
+    s->cv_work.notify_all();
+  }
 }
 
 constexpr size_t kMaxLatencySamples = size_t(1) << 22;
@@ -211,8 +236,14 @@ bool ss_server::launch_slot(Slot &sl, std::unique_lock<std::mutex> &lk) {
          cudaMemcpyAsync(sl.h_status, sl.d_status, nb * sizeof(int32_t),
                          cudaMemcpyDeviceToHost, sl.stream) == cudaSuccess;
   sl.launch_failed = !ok;
-  if (cudaLaunchHostFunc(sl.stream, slot_done_cb, &sl) != cudaSuccess) {
-    // no callback will come: complete the slot here (as failed)
+  if (cudaEventRecord(sl.done_ev, sl.stream) == cudaSuccess) {
+    {
+      std::lock_guard<std::mutex> wl(sl.wmu);
+      sl.armed = true;
+    }
+    sl.wcv.notify_one();
+  } else {
+    // nothing will signal this launch: complete the slot here (as failed)
     sl.launch_failed = true;
     sl.t_done = Clock::now();
     sl.done.store(true, std::memory_order_release);
@@ -275,8 +306,44 @@ int ss_server::submit_at(const float *query, int K, int L, Clock::time_point t_a
   return SS_OK;
 }
 
+int ss_server::submit_many(const float *queries, const int32_t *Ks, const int32_t *Ls,
+                           const Clock::time_point *t_arrival, uint32_t count,
+                           uint64_t *tickets) {
+  for (uint32_t i = 0; i < count; ++i)
+    if (Ks[i] < 1 || Ks[i] > Ls[i] || Ks[i] > cfg.K_max || Ls[i] > cfg.L_max)
+      return -ssb::index_error(h, SS_ERR_INVALID_ARGUMENT,
+                               "request needs 1 <= K <= L, K <= K_max and L <= L_max");
+  uint32_t n = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (stop) return -ssb::index_error(h, SS_ERR_INVALID_ARGUMENT, "server is stopping");
+    for (; n < count && next_ticket - oldest < cap; ++n) {
+      const uint64_t t = next_ticket++;
+      Request &r = req(t);
+      std::memcpy(&ring_q[(t % cap) * dim], queries + (size_t)n * dim, (size_t)dim * sizeof(float));
+      r.K = Ks[n];
+      r.L = Ls[n];
+      r.t_arrival = t_arrival[n];
+      r.state = kPending;
+      ++n_submitted;
+      tickets[n] = t + 1;  // tickets handed out start at 1
+    }
+  }
+  if (n) cv_work.notify_all();
+  return (int)n;
+}
+
 void ss_server::free_slots() {
   for (auto &sl : slots) {
+    if (sl->waiter.joinable()) {
+      {
+        std::lock_guard<std::mutex> wl(sl->wmu);
+        sl->quit = true;
+      }
+      sl->wcv.notify_one();
+      sl->waiter.join();
+    }
+    if (sl->done_ev) cudaEventDestroy(sl->done_ev);
     if (sl->stream) cudaStreamDestroy(sl->stream);
     cudaFree(sl->d_q);
     cudaFree(sl->d_dists);
@@ -354,6 +421,8 @@ int ss_server_create(ss_index *h, const ss_server_config *cfg, ss_server **out) 
     auto sl = std::make_unique<Slot>();
     sl->owner = s.get();
     ok = cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreateWithFlags(&sl->done_ev,
+                                  cudaEventDisableTiming | cudaEventBlockingSync) == cudaSuccess &&
          dev_alloc(&sl->d_q, B * s->dim) == cudaSuccess &&
          dev_alloc(&sl->d_K, B) == cudaSuccess && dev_alloc(&sl->d_L, B) == cudaSuccess &&
          dev_alloc(&sl->d_off, B) == cudaSuccess && dev_alloc(&sl->d_ids, B * Kx) == cudaSuccess &&
@@ -373,6 +442,7 @@ int ss_server_create(ss_index *h, const ss_server_config *cfg, ss_server **out) 
   }
   cudaSetDevice(prev);
   ss_server *raw = s.get();
+  for (auto &sl : raw->slots) sl->waiter = std::thread(slot_waiter, sl.get(), raw->device);
   raw->dispatcher = std::thread([raw] { raw->run(); });
   *out = s.release();
   return SS_OK;
@@ -419,32 +489,40 @@ int ss_server_replay(ss_server *s, const float *queries, uint32_t nq, const int3
   std::vector<int64_t> off(nq, 0);
   for (uint32_t i = 1; i < nq; ++i) off[i] = off[i - 1] + Ks[i - 1];
   std::atomic<int> gen_rc{SS_OK};
-  // The generator sleeps until each arrival time and then submits every
-  // request that is due (it never spins: a busy client thread competes with
-  // the dispatcher for the host's cores); latency still runs from the
-  // scheduled arrival, so a late wake-up counts against the server.
+  // The generator sleeps until the next arrival time and then submits every
+  // request that is due in one go (it never spins: a busy client thread
+  // competes with the dispatcher for the host's cores); latency still runs
+  // from each request's scheduled arrival, so a late wake-up counts against
+  // the server.
   std::mutex sub_mu;
   std::condition_variable sub_cv;
   uint32_t submitted = 0;
   const Clock::time_point t0 = Clock::now();
+  std::vector<Clock::time_point> t_arr(nq);
+  for (uint32_t i = 0; i < nq; ++i)
+    t_arr[i] = t0 + std::chrono::duration_cast<Clock::duration>(
+                        std::chrono::duration<double, std::micro>(arrival_us[i]));
   std::thread gen([&] {
-    for (uint32_t i = 0; i < nq; ++i) {
-      const auto t_arr = t0 + std::chrono::duration_cast<Clock::duration>(
-                                  std::chrono::duration<double, std::micro>(arrival_us[i]));
-      if (Clock::now() < t_arr) std::this_thread::sleep_until(t_arr);
-      int rc;
-      for (;;) {
-        rc = s->submit_at(queries + (size_t)i * s->dim, Ks[i], Ls[i], t_arr, &tickets[i]);
-        if (rc != SS_ERR_BUSY) break;
-        std::this_thread::sleep_for(std::chrono::microseconds(50));
-      }
-      if (rc != SS_OK) gen_rc.store(rc);
-      {
+    uint32_t i = 0;
+    while (i < nq) {
+      if (Clock::now() < t_arr[i]) std::this_thread::sleep_until(t_arr[i]);
+      const Clock::time_point now = Clock::now();
+      uint32_t due = i + 1;
+      while (due < nq && t_arr[due] <= now && due - i < 4096) ++due;
+      const int n = s->submit_many(queries + (size_t)i * s->dim, Ks + i, Ls + i, t_arr.data() + i,
+                                   due - i, tickets.data() + i);
+      if (n < 0) {
+        gen_rc.store(-n);
         std::lock_guard<std::mutex> lk(sub_mu);
-        submitted = rc == SS_OK ? i + 1 : nq + 1;  // nq + 1: stopped early
+        submitted = nq + 1;  // stopped early
+      } else {
+        i += (uint32_t)n;
+        std::lock_guard<std::mutex> lk(sub_mu);
+        submitted = i;
       }
       sub_cv.notify_one();
-      if (rc != SS_OK) break;
+      if (n < 0) break;
+      if (n == 0) std::this_thread::sleep_for(std::chrono::microseconds(50));  // ring full
     }
   });
   int rc = SS_OK;
