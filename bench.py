@@ -209,22 +209,27 @@ class ClockSampler:
 
 
 PROFILED_TRAFFIC = {
-    # (workload, L, queries) -> ncu summary holding the DRAM bytes of one launch
-    ("cfg3", 400, 10000): "profiles/warp_search_kernel_1.2Mx200_ip_L400.md",
+    # workload -> ncu summary holding the DRAM bytes per row evaluated on the
+    # device, measured on one launch of a smaller case of the same kernel and
+    # layout whose base is well above L2
+    "cfg3": "profiles/warp_search_kernel_900kx200_ip_L400_dram.md",
 }
 
 
-def profiled_traffic(workload, L, nq):
-    """DRAM bytes (read + write) of one search launch from the committed ncu
-    summary of this exact workload, or None when none was captured."""
-    rel = PROFILED_TRAFFIC.get((workload, L, nq))
+def profiled_traffic(workload, device_rows):
+    """DRAM bytes (read + write) of one search launch: the committed small-case
+    ncu figure per evaluated row times the rows this launch evaluated on the
+    device, or None when no capture exists for the workload."""
+    rel = PROFILED_TRAFFIC.get(workload)
     if not rel:
         return None, None
     try:
         with open(os.path.join(ROOT, rel)) as f:
             for line in f:
-                if line.startswith("traffic_bytes_per_launch:"):
-                    return float(line.split(":", 1)[1]), rel
+                if line.startswith("traffic_bytes_per_evaluated_row:"):
+                    per_row = float(line.split(":", 1)[1])
+                    return per_row * float(device_rows), (
+                        f"{rel}: {per_row:.1f} B per evaluated row x {int(device_rows)} rows")
     except OSError:
         pass
     return None, None
@@ -899,7 +904,8 @@ def run_ours(args):
         if solo and not args.no_config1 and args.workload == "cfg3" and args.scale == 1.0 else None
 
     peak, peak_kind = measured_hbm_peak()
-    traffic, traffic_src = profiled_traffic(args.workload, L, nq)
+    traffic, traffic_src = profiled_traffic(args.workload, ndc_dev.sum()) \
+        if args.scale == 1.0 and L == 400 else (None, None)
     mean_step_s = sum(step_ms) / len(step_ms) / 1000.0
     achieved = bytes_per_step / mean_step_s / 1e9
 
@@ -1086,7 +1092,7 @@ def run_uneven(args):
     plain_qps = ns / (time.perf_counter() - t0)
 
     peak, peak_kind = measured_hbm_peak()
-    traffic, traffic_src = profiled_traffic(args.workload, L_max, nq)
+    traffic, traffic_src = profiled_traffic(args.workload, ndc_dev.sum())
     mean_step_s = sum(step_ms) / len(step_ms) / 1000.0
     achieved = bytes_per_step / mean_step_s / 1e9
     out = {
