@@ -225,7 +225,7 @@ int status_counts_to_error(ss_index *h, const uint32_t *counts, uint32_t first) 
   const uint32_t timeout = counts[ssb::kStatusStageTimeout];
   if (timeout)
     return set_err(h, SS_ERR_TIMEOUT,
-                   "%u queries gave up waiting for a free row stage (first failed query: %u); "
+                   "%u queries gave up waiting for their row copies (first failed query: %u); "
                    "results are invalid", timeout, first);
   if (hop)
     return set_err(h, SS_ERR_SEARCH_LIMIT, "%u queries hit the hop limit (first failed query: %u)",

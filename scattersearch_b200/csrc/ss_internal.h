@@ -66,7 +66,7 @@ enum : int32_t {
   kStatusBadArgs = 1,
   kStatusHopLimit = 2,
   kStatusVisitedFull = 3,
-  kStatusStageTimeout = 4,  // no row stage of the CTA's shared pool became free within its wait limit
+  kStatusStageTimeout = 4,  // a shared-memory row stage was not filled within its wait limit
   kStatusKinds = 5          // number of status codes
 };
 

@@ -16,8 +16,8 @@
 //                        from a device work counter until the batch is empty
 //                        (persistent) or take them by index (static).  Base
 //                        rows reach each team through a row stage filled by
-//                        asynchronous 16-byte copies: a team's own stage, or
-//                        one taken from a pool the CTA's teams share.  Stages deeper than 16
+//                        bulk copies: a team's own stage, or one taken from a
+//                        pool the CTA's teams share.  Stages deeper than 16
 //                        rows (one copy round trip per hop) are a separate
 //                        instantiation (DEEP), used for launches small
 //                        enough to keep every query resident.
@@ -44,9 +44,9 @@ namespace {
 
 constexpr uint32_t kExplored = 0x80000000u;
 // Most rows staged in shared memory per pass of the warp kernel (one per
-// lane pair), and the iteration limit of a wait for a free stage of a CTA's
-// shared pool (a stage is held for microseconds; the limit is far above that
-// and only ends a wait that would never finish).
+// lane pair), and the iteration limit of a wait for them (a stage load takes
+// microseconds; the limit is far above that and only ends a wait that would
+// never finish).
 constexpr int kStageRows = 16;
 // Deepest whole-row stage: a hop has at most 32 fresh candidates (degree
 // <= 32 with one adjacency chunk), so a 32-row stage takes every row of a
@@ -296,8 +296,8 @@ __device__ __forceinline__ int floor_pow2(int n) { return n > 0 ? 1 << (31 - __c
 // that it starts on a 128-byte boundary (every team's region is a multiple of
 // 128 bytes).
 struct WarpSmem {
-  float *stage;                    // stage_rows base rows (nb*8 floats each), filled by cp.async
-  uint64_t *bar;                   // 4 words after a private stage, reserved
+  float *stage;                    // stage_rows base rows (nb*8 floats each), filled by TMA
+  uint64_t *bar;                   // mbarrier of the stage
   float *q;
   uint32_t *pk, *pid;              // pool keys / ids (bit 31 of id = explored)
   uint32_t *cid, *ckey;            // this hop's fresh candidates, adjacency order
@@ -312,7 +312,7 @@ __device__ __forceinline__ WarpSmem carve_warp(uint32_t *base, const SmemPlan &p
     base += p.stage_words;
     s.bar = reinterpret_cast<uint64_t *>(base);
     base += 4;
-  } else {  // the CTA's stage pool holds the stages
+  } else {  // the CTA's stage pool holds the stages and their mbarriers
     s.stage = nullptr;
     s.bar = nullptr;
   }
@@ -336,27 +336,44 @@ __device__ __forceinline__ uint32_t smem_addr(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-// Row stage of one team: base rows are copied into shared memory with
-// asynchronous 16-byte copies (cp.async.cg, L2 only), the 32 lanes of the
-// team covering consecutive 16-byte pieces of a row, so one warp instruction
-// moves up to 512 contiguous bytes and a row reaches DRAM as whole sectors
-// in a burst.  Each lane waits for its own copies (cp.async.wait_group, a
-// hardware wait), then the warp synchronises.  Copying a row with one
-// cp.async.bulk instead cost about 100 cycles of issue per row, over 2,000
-// cycles a hop with two copy passes.
+// Bounded wait for phase `parity` of a shared-memory mbarrier; false when the
+// iteration limit ran out first.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (uint32_t spin = 0; spin < kStageWaitLimit; ++spin) {
+    uint32_t done;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// Row stage of one team: base rows are copied whole into shared memory by
+// the bulk-copy (TMA) engine, one cp.async.bulk per row, completing on the
+// team's mbarrier.  A row requested as one 16-byte-aligned block reaches
+// DRAM as one burst per row, which a random gather needs to approach the
+// HBM copy rate; rows read by many lanes a sector at a time do not.
 struct RowStage {
+  uint32_t bar;     // shared address of the mbarrier
+  uint32_t phase;   // parity of the phase being filled
+  bool broken;      // a wait timed out: the stage may still be written to
   float *buf;       // the stage's rows
   int slot;         // pool slot held (shared stages), -1 when none
 };
 
 // Stage pool of a CTA whose teams share row stages (SmemPlan::shared_stages
-// > 0): `count` stages and a bit mask of free stages (3 words per stage
-// after the stages are reserved, then the mask).  A team takes a stage just before it
+// > 0): `count` stages, each with its mbarrier and the parity of its next
+// phase, and a bit mask of free stages.  A team takes a stage just before it
 // starts copying rows and gives it back once the distances of its last pass
 // are computed, so a stage is held only over copy latency and distance
 // arithmetic and the CTA needs fewer stages than teams.
 struct StagePool {
   float *stages;      // count x stage_words floats
+  uint32_t bar0;      // shared address of the first mbarrier (8 bytes apart)
+  uint32_t *phases;   // count words
   uint32_t *mask;     // bit i set = stage i free
   uint32_t count, stage_words;
 };
@@ -373,7 +390,10 @@ __device__ __forceinline__ StagePool carve_pool(uint32_t *base, const SmemPlan &
   sp.count = p.shared_stages;
   sp.stage_words = p.stage_words;
   sp.stages = reinterpret_cast<float *>(base);
-  sp.mask = base + p.shared_stages * p.stage_words + 3 * p.shared_stages;
+  uint32_t *b = base + p.shared_stages * p.stage_words;  // 8-byte aligned (stage_words % 32 == 0)
+  sp.bar0 = (uint32_t)__cvta_generic_to_shared(b);
+  sp.phases = b + 2 * p.shared_stages;
+  sp.mask = sp.phases + p.shared_stages;
   return sp;
 }
 
@@ -384,6 +404,7 @@ __device__ __forceinline__ StagePool carve_pool(uint32_t *base, const SmemPlan &
 __device__ __forceinline__ bool stage_acquire(RowStage &st, const StagePool &sp, int lane) {
   if (sp.count == 0 || st.slot >= 0) return true;
   int got = -1;
+  uint32_t phase = 0;
   if (lane == 0) {
     volatile uint32_t *vm = sp.mask;
     for (uint32_t spin = 0; spin < kStageWaitLimit && got < 0; ++spin) {
@@ -395,12 +416,18 @@ __device__ __forceinline__ bool stage_acquire(RowStage &st, const StagePool &sp,
       const int i = __ffs(m) - 1;
       if (atomicCAS(sp.mask, m, m & ~(1u << i)) == m) got = i;
     }
-    if (got >= 0) __threadfence_block();  // the previous holder's reads come first
+    if (got >= 0) {
+      __threadfence_block();
+      phase = *(volatile uint32_t *)(sp.phases + got);
+    }
   }
   got = __shfl_sync(kFull, got, 0);
+  phase = __shfl_sync(kFull, phase, 0);
   if (got < 0) return false;
   st.slot = got;
   st.buf = sp.stages + (size_t)got * sp.stage_words;
+  st.bar = sp.bar0 + 8u * (uint32_t)got;
+  st.phase = phase;
   return true;
 }
 
@@ -411,6 +438,8 @@ __device__ __forceinline__ void stage_release(RowStage &st, const StagePool &sp,
   __syncwarp();
   if (lane == 0) {
     // this team's reads of the stage come before any later copy into it
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    *(volatile uint32_t *)(sp.phases + st.slot) = st.phase;
     __threadfence_block();
     atomicOr(sp.mask, 1u << st.slot);
   }
@@ -421,45 +450,61 @@ __device__ __forceinline__ void stage_release(RowStage &st, const StagePool &sp,
 // tail block (processed first, distance.cpp:42-45) plus the leading blocks.
 __host__ __device__ __forceinline__ uint32_t split_first(uint32_t nb) { return (nb + 1) / 2; }
 
-__device__ __forceinline__ void cp_async16(float *dst, const float *src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src)
-               : "memory");
-}
-
 // Starts copying part `part` of the base rows of cid[0..m) (m <= the stage's
 // rows) into the stage: part 2 is the whole row (memory order); with a split
 // stage, part 0 is the first half of the blocks in processing order (the odd
-// tail block, then blocks 0, 1, ...) and part 1 the rest.  A row's 32-byte
-// blocks are two 16-byte pieces each, handed to consecutive lanes.  All 32
-// lanes call it; cid must be visible to every lane.
-template <int NB>
-__device__ __forceinline__ void stage_issue(const GraphView &g, const RowStage &st,
+// tail block, then blocks 0, 1, ...) and part 1 the rest.  All 32 lanes call
+// it; cid must be visible to every lane.
+__device__ __forceinline__ void stage_issue(const GraphView &g, const WarpSmem &s, const RowStage &st,
                                             const uint32_t *cid, int m, int part, uint32_t row_words,
                                             int lane) {
-  const uint32_t nb = NB > 0 ? (uint32_t)NB : g.nb, A = split_first(nb);
+  const uint32_t nb = g.nb, A = split_first(nb);
   const bool odd = nb & 1u;
-  const uint32_t nblk = part == 2 ? nb : (part == 0 ? A : nb - A);
-  const uint32_t pieces = 2u * nblk;
-  __syncwarp();  // every lane's reads of the stage come before the copies over it
-  for (int r = 0; r < m; ++r) {
-    const float *row = g.base + (size_t)cid[r] * (size_t)(nb * 8);
-    float *dst = st.buf + (size_t)r * row_words;
-    for (uint32_t c = lane; c < pieces; c += 32) {
-      const uint32_t k = c >> 1, half = (c & 1u) * 4u;  // staged block, 16-byte piece
-      const uint32_t sb = part == 2 ? k
-                          : part == 0 ? (odd ? (k == 0 ? nb - 1 : k - 1) : k)
-                                      : (odd ? A - 1 : A) + k;
-      cp_async16(dst + k * 8 + half, row + sb * 8 + half);
-    }
+  uint32_t bytes, src_block, dst_block = 0, nblocks;
+  if (part == 2) {
+    nblocks = nb;
+    src_block = 0;
+  } else if (part == 0) {
+    nblocks = odd ? A - 1 : A;
+    src_block = 0;
+    dst_block = odd ? 1 : 0;
+  } else {
+    nblocks = nb - A;
+    src_block = odd ? A - 1 : A;
   }
-  asm volatile("cp.async.commit_group;" ::: "memory");
+  bytes = (nblocks + (part == 0 && odd ? 1u : 0u)) * 32u;
+  // earlier reads of the stage (generic proxy) come before the copies that
+  // overwrite it (async proxy)
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if (lane == 0)
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(st.bar),
+                 "r"(bytes * (uint32_t)m)
+                 : "memory");
+  __syncwarp();
+  if (lane < m) {
+    const float *row = g.base + (size_t)cid[lane] * (size_t)(nb * 8);
+    float *dst = st.buf + lane * row_words;
+    if (nblocks > 0)
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+              smem_addr(dst + dst_block * 8)),
+          "l"(row + src_block * 8), "r"(nblocks * 32u), "r"(st.bar)
+          : "memory");
+    if (part == 0 && odd)
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+              smem_addr(dst)),
+          "l"(row + (nb - 1) * 8), "r"(32u), "r"(st.bar)
+          : "memory");
+  }
 }
 
-// Waits for the copies of stage_issue: each lane for its own pieces, then the
-// warp, so every lane sees every row.
-__device__ __forceinline__ void stage_wait() {
-  asm volatile("cp.async.wait_group 0;" ::: "memory");
-  __syncwarp();
+// Waits for the copies of stage_issue.  Returns false on a timed-out wait.
+__device__ __forceinline__ bool stage_wait(RowStage &st) {
+  const bool ok = mbar_wait(st.bar, st.phase);
+  st.phase ^= 1u;
+  if (!ok) st.broken = true;
+  return __all_sync(kFull, ok);
 }
 
 // Lane-pair accumulation over processing steps [T0, T1) of the reference
@@ -521,7 +566,7 @@ __device__ __forceinline__ float pair_finish(const GraphView &g, int h, float a0
 // loads the first halves, accumulates, then loads the second halves (L2
 // hits) into the same buffer.  When `first_issued`, the first load (part 0,
 // or the whole rows) was already started with stage_issue.  Returns false
-// when no stage of the CTA's pool became free within the wait limit.
+// when a stage wait timed out.
 template <int NB, bool DEEP>
 __device__ __forceinline__ bool eval_staged(const GraphView &g, const WarpSmem &s, RowStage &st,
                                             const StagePool &sp, const SmemPlan &p,
@@ -540,8 +585,8 @@ __device__ __forceinline__ bool eval_staged(const GraphView &g, const WarpSmem &
     if constexpr (DEEP) {  // stages deeper than 16 rows: one wait, 16-row groups
       if (!split) {
         if (p0 > 0 || !first_issued)
-          stage_issue<NB>(g, st, cid + p0, m, 2, p.stage_row_words, lane);
-        stage_wait();
+          stage_issue(g, s, st, cid + p0, m, 2, p.stage_row_words, lane);
+        if (!stage_wait(st)) return false;
         for (int g0 = 0; g0 < m; g0 += 16) {
           const int mg = min(16, m - g0);
           const float *rowg = st.buf + (g0 + (c < mg ? c : 0)) * p.stage_row_words;
@@ -557,16 +602,16 @@ __device__ __forceinline__ bool eval_staged(const GraphView &g, const WarpSmem &
     const float *row = st.buf + (c < m ? c : 0) * p.stage_row_words;
     float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
     if (!split) {
-      if (p0 > 0 || !first_issued) stage_issue<NB>(g, st, cid + p0, m, 2, p.stage_row_words, lane);
-      stage_wait();
+      if (p0 > 0 || !first_issued) stage_issue(g, s, st, cid + p0, m, 2, p.stage_row_words, lane);
+      if (!stage_wait(st)) return false;
       staged_accumulate<NB, true>(g, s.q, row, h, 0, nb, a0, a1, a2, a3);
     } else {
-      if (p0 > 0 || !first_issued) stage_issue<NB>(g, st, cid + p0, m, 0, p.stage_row_words, lane);
-      stage_wait();
+      if (p0 > 0 || !first_issued) stage_issue(g, s, st, cid + p0, m, 0, p.stage_row_words, lane);
+      if (!stage_wait(st)) return false;
       staged_accumulate<NB, false>(g, s.q, row, h, 0, A, a0, a1, a2, a3);
       __syncwarp();
-      stage_issue<NB>(g, st, cid + p0, m, 1, p.stage_row_words, lane);
-      stage_wait();
+      stage_issue(g, s, st, cid + p0, m, 1, p.stage_row_words, lane);
+      if (!stage_wait(st)) return false;
       staged_accumulate<NB, false>(g, s.q, row, h, A, nb, a0, a1, a2, a3);
     }
     const float d = pair_finish(g, h, a0, a1, a2, a3);
@@ -891,7 +936,7 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
       if (RCH == 1 && nc > 0) {
         __syncwarp();
         if (stage_acquire(st, sp, lane)) {
-          stage_issue<NB>(g, st, s.cid, min(nc, srows), p.stage_split > 1 ? 0 : 2,
+          stage_issue(g, s, st, s.cid, min(nc, srows), p.stage_split > 1 ? 0 : 2,
                       p.stage_row_words, lane);
           issued = true;
         }
@@ -976,13 +1021,29 @@ __global__ void __launch_bounds__(256, 2) warp_search_kernel(GraphView g, BatchA
   const StagePool sp = carve_pool(smem, p);
   const WarpSmem s = carve_warp(smem + stage_pool_words(p) + (size_t)warp * p.words_per_team, p);
   RowStage st;
+  st.phase = 0;
+  st.broken = false;
   if (p.shared_stages == 0) {  // a private stage, always held
+    st.bar = smem_addr(s.bar);
     st.buf = s.stage;
     st.slot = 0;
+    if (lane == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(st.bar) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
   } else {  // the CTA's stage pool
+    st.bar = 0;
     st.buf = nullptr;
     st.slot = -1;
-    if (threadIdx.x == 0) *sp.mask = sp.count >= 32 ? ~0u : ((1u << sp.count) - 1u);
+    if (threadIdx.x == 0) {
+      for (uint32_t i = 0; i < sp.count; ++i) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sp.bar0 + 8u * i) : "memory");
+        sp.phases[i] = 0u;
+      }
+      *sp.mask = sp.count >= 32 ? ~0u : ((1u << sp.count) - 1u);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     __syncthreads();
   }
   const uint32_t slot = blockIdx.x * wpb + warp;
@@ -1005,6 +1066,12 @@ __global__ void __launch_bounds__(256, 2) warp_search_kernel(GraphView g, BatchA
                                a.dists ? a.dists + off : nullptr, a.ndc ? a.ndc + q : nullptr,
                                a.hops ? a.hops + q : nullptr, a.status ? a.status + q : nullptr, s,
                                p, st, sp, a.max_hops, lane);
+      // a stage copy that never completed leaves this team's stage unusable:
+      // wait once more (bounded) for it and take no further queries
+      if (st.broken) {
+        mbar_wait(st.bar, st.phase ^ 1u);
+        break;
+      }
     }
     if (!a.work_counter) q += nslots;
   }
