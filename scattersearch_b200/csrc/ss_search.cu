@@ -698,10 +698,13 @@ __device__ __forceinline__ void accepted_positions(const WarpSmem &s, int na, in
 // repeats an id across chunks would otherwise offer it twice, where the
 // reference's visited flags skip the second occurrence (annsearch.cpp:229-231).
 // Both copies have the same key, so the first one is accepted iff the second
-// would be.  Returns the count.
+// would be.  `chunk_dups` asks for the same check among the candidates of one
+// 32-candidate chunk; only a list that can hold repeats needs it (rows wider
+// than 32, entries copied from another pool).  Returns the count.
 template <int RCH>
 __device__ __forceinline__ int accept_candidates(const WarpSmem &s, int nc, int size, uint32_t thr,
-                                                 bool check_dups, int lane) {
+                                                 bool check_dups, int lane,
+                                                 bool chunk_dups = false) {
   const unsigned lanemask_lt = (1u << lane) - 1u;
   const int top = floor_pow2(size);
   int na = 0;
@@ -728,7 +731,7 @@ __device__ __forceinline__ int accept_candidates(const WarpSmem &s, int nc, int 
         }
       }
     }
-    if (check_dups) {
+    if (chunk_dups) {
       // copies of one id in this 32-candidate chunk (the fresh ids of a row's
       // chunks are compacted, so they need not sit in different chunks
       // here): the first in adjacency order stays
@@ -982,7 +985,8 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
     // 4. acceptance in adjacency order, with each key's pool rank; after an
     //    eviction, a candidate already in the pool (same id under the same
     //    key) is dropped
-    const int na = accept_candidates<RCH>(s, nc, size, thr, vis.lossy, lane);
+    const int na = accept_candidates<RCH>(s, nc, size, thr, vis.lossy, lane,
+                                          RCH > 1 && vis.lossy);
     if (na == 0) {
       pref_node = unode;
       if (unode != kNoneId) load_row<RCH>(g, unode, lane, pref_row);
@@ -1794,7 +1798,7 @@ __global__ void __launch_bounds__(512) scatter_search_kernel(GraphView g, BatchA
           left -= got;
           if (got == 0) continue;
           const uint32_t thr = s.pk[size - 1];
-          const int na = accept_candidates<RCH>(s, got, size, thr, true, lane);
+          const int na = accept_candidates<RCH>(s, got, size, thr, true, lane, true);
           if (na == 0) continue;
           __syncwarp();
           uint32_t nkey[RCH], nid[RCH];
