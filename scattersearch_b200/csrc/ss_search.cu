@@ -560,11 +560,9 @@ __device__ __forceinline__ float pair_finish(const GraphView &g, int h, float a0
   return g.metric == 0 ? r : -r;
 }
 
-// Keys of cid[0..nc) into ckey[0..nc), one distance per lane pair.  The
-// first `srows` rows (<= 16) come through the row stage; with a whole-row
-// stage the rest are sent to L2 first and read directly by the lane pairs,
-// 16 rows a pass (stages deeper than 16 rows take every row of a hop in one
-// copy round trip).  With a split stage every row is prefetched, and each pass
+// Keys of cid[0..nc) into ckey[0..nc) in passes of `srows` rows (<= 16),
+// one distance per lane pair.  With a whole-row stage, rows beyond the first
+// pass are sent to L2 first; with a split stage every row is, and each pass
 // loads the first halves, accumulates, then loads the second halves (L2
 // hits) into the same buffer.  When `first_issued`, the first load (part 0,
 // or the whole rows) was already started with stage_issue.  Returns false
@@ -600,21 +598,6 @@ __device__ __forceinline__ bool eval_staged(const GraphView &g, const WarpSmem &
         __syncwarp();
         continue;
       }
-    }
-    if (!DEEP && !split && p0 > 0) {
-      // Rows beyond the first pass were prefetched to L2 at the start: each
-      // lane pair reads its row straight from global memory (16 rows a pass)
-      // instead of staging it, which saves a round of bulk-copy issue
-      // (about 100 cycles a row) and a stage wait.
-      stage_release(st, sp, lane);
-      for (int q0 = p0; q0 < nc; q0 += 16) {
-        const int j = q0 + c;
-        const bool act = j < nc;
-        const float d = pair_distance<NB>(g, s.q, act ? cid[j] : 0u, act, h);
-        if (h == 0 && act) ckey[j] = float_to_key(d);
-      }
-      __syncwarp();
-      return true;
     }
     const float *row = st.buf + (c < m ? c : 0) * p.stage_row_words;
     float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
