@@ -287,6 +287,14 @@ int ss_set_tuning(ss_index *h, int warps_per_block, int hash_cap, int blocks_per
  * never depend on either. */
 int ss_set_stage_layout(ss_index *h, int stage_rows, int stages_per_block);
 
+/* How the batched kernel fills its row stages.  SS_ROW_COPY_AUTO: four rows
+ * per tensor-map gather copy (cp.async.bulk.tensor tile::gather4) when a row
+ * has at most 256 floats and a stage holds a multiple of 4 rows, else one
+ * bulk copy per row; SS_ROW_COPY_BULK: always one bulk copy per row.
+ * Results never depend on it. */
+enum { SS_ROW_COPY_AUTO = 0, SS_ROW_COPY_BULK = 1 };
+int ss_set_row_copy(ss_index *h, int mode);
+
 /* ---- exact brute force -------------------------------------------------- */
 
 /* Exact k nearest base rows of each query by brute force (no graph needed);

@@ -369,6 +369,15 @@ class ANNSearch:
                                             int(blocks_per_sm_cap)))
         self._check(self._lib.ss_set_stage_layout(self._h, int(stage_rows), int(shared_stages)))
 
+    ROW_COPY_AUTO = 0
+    ROW_COPY_BULK = 1
+
+    def set_row_copy(self, mode: int = 0):
+        """How the batched kernel fills its row stages (ss_set_row_copy):
+        ROW_COPY_AUTO, four rows per gather4 tensor copy where rows allow it,
+        or ROW_COPY_BULK, one bulk copy per row; never changes results."""
+        self._check(self._lib.ss_set_row_copy(self._h, int(mode)))
+
 
 class SearchPlan:
     """A graph-captured batched search (ss_plan_*): ``launch(stream)``

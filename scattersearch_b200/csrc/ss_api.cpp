@@ -121,6 +121,7 @@ struct ss_index {
   int blocks_per_sm_cap = 0;
   int shared_stages = 0;  // row stages shared by a CTA's teams (0 = one per team)
   int stage_rows = 0;     // rows per row stage (0 = 16)
+  int row_copy = SS_ROW_COPY_AUTO;  // how row stages are filled (ss_set_row_copy)
 
   ssb::GraphView view() const {
     ssb::GraphView g;
@@ -320,12 +321,14 @@ ssb::SmemPlan plan_launch(ss_index *h, const ssb::GraphView &g, int L_max, uint3
       }
       if (nq <= limit) {
         *wpb = w;
+        if (h->row_copy == SS_ROW_COPY_BULK) p.gather = 0;
         return p;
       }
     }
   }
   ssb::SmemPlan p = ssb::plan_warp_smem(g, L_max, h->hash_cap_override, h->stage_rows);
   *wpb = choose_wpb(h, p, true);
+  if (h->row_copy == SS_ROW_COPY_BULK) p.gather = 0;
   return p;
 }
 
@@ -1303,6 +1306,14 @@ int ss_set_stage_layout(ss_index *h, int stage_rows, int stages_per_block) {
     return set_err(h, SS_ERR_INVALID_ARGUMENT, "stages_per_block must be in [0, 32]");
   h->stage_rows = stage_rows;
   h->shared_stages = stages_per_block;
+  return SS_OK;
+}
+
+int ss_set_row_copy(ss_index *h, int mode) {
+  if (!h) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null index handle");
+  if (mode != SS_ROW_COPY_AUTO && mode != SS_ROW_COPY_BULK)
+    return set_err(h, SS_ERR_INVALID_ARGUMENT, "unknown row copy mode %d", mode);
+  h->row_copy = mode;
   return SS_OK;
 }
 

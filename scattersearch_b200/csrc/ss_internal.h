@@ -57,6 +57,7 @@ struct SmemPlan {
   uint32_t stage_row_words;  // warp kernel: floats per staged row
   uint32_t stage_words; // warp kernel: size of the row stage
   uint32_t shared_stages;  // warp kernel: row stages shared by a CTA's teams (0 = one per team)
+  uint32_t gather;      // warp kernel: whole rows staged by gather4 copies (set at launch)
   uint32_t words_per_team;
 };
 
@@ -84,6 +85,9 @@ SmemPlan plan_intra_smem(const GraphView &g, int L_max, int width, int hash_cap_
 // Launch helpers.  Return cudaSuccess or the launch error.
 //   warps_per_block: teams per CTA; blocks: grid size (0 = one per team
 //   needed for nq with a static schedule).
+// Stages whole rows with gather4 copies when p.gather is set and the base
+// rows encode as a tensor map (rows of at most 256 floats, 16-byte aligned
+// base); otherwise with one bulk copy per row.
 cudaError_t launch_warp_search(const GraphView &g, const BatchArgs &a, const SmemPlan &p,
                                int warps_per_block, int blocks, cudaStream_t stream);
 cudaError_t launch_intra_search(const GraphView &g, const BatchArgs &a, const SmemPlan &p,

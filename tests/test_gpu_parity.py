@@ -486,3 +486,32 @@ def test_small_launches_and_deep_stages_keep_results(oracle_lib, name):
         assert _same_bits(t_d, np.tile(d, (reps, 1))), (wpb, stages, rows)
     idx.set_tuning()
     idx.close()
+
+
+@pytest.mark.parametrize("dim,metric", [(200, 1), (96, 0), (256, 0), (13, 1)])
+def test_gather_and_bulk_row_copies_agree(oracle_lib, dim, metric):
+    """Row stages filled four rows per gather4 tensor copy (rows of at most
+    256 floats, the default) and one bulk copy per row return the same ids
+    and distance bits, in private and shared stages of 12, 16, 24 and 32
+    rows, and both match the oracle.  Stages of a row count that is not a
+    multiple of 4 (17) take bulk copies in either mode."""
+    O = oracle_lib
+    X, Q, adj, ep = _synthetic(dim + 7, 4000, dim, 32, metric)
+    idx = _index(X, adj, ep, metric)
+    K, L = 10, 128
+    o_ids, o_d, _, _ = O.search(X, adj, ep, metric, Q, K, L)
+    big = _tile(Q)
+    reps = len(big) // len(Q)
+    for wpb, stages, rows in ((2, 0, 12), (4, 3, 16), (2, 0, 24), (4, 2, 32), (1, 0, 17)):
+        idx.set_tuning(warps_per_block=wpb, shared_stages=stages, stage_rows=rows)
+        for mode in (idx.ROW_COPY_AUTO, idx.ROW_COPY_BULK):
+            idx.set_row_copy(mode)
+            ids, d = idx.search_batch(big, K, L)
+            assert np.array_equal(ids, np.tile(o_ids, (reps, 1))), (dim, wpb, stages, rows, mode)
+            assert _same_bits(d, np.tile(o_d, (reps, 1))), (dim, wpb, stages, rows, mode)
+    idx.set_row_copy(idx.ROW_COPY_AUTO)
+    idx.set_tuning()
+    # small launches take the latency layout (32-row stages)
+    ids, d = idx.search_batch(Q[:20], K, L)
+    assert np.array_equal(ids, o_ids[:20]) and _same_bits(d, o_d[:20])
+    idx.close()
