@@ -282,6 +282,27 @@ __device__ __forceinline__ void prefetch_rows(const GraphView &g, const uint32_t
   }
 }
 
+// Starts an L2 prefetch of the base rows of cid[0..nc) through the row map,
+// four rows per gather4 prefetch (group j = rows 4j..4j+3, taken by lane
+// j mod 32; a short last group repeats its first row).  One instruction per
+// four rows, against about 77 line prefetches for 11 rows of 800 bytes.
+__device__ __forceinline__ void prefetch_rows_gather(const CUtensorMap *rows, const uint32_t *cid,
+                                                     int nc, int lane) {
+  const int groups = (nc + 3) >> 2;
+  for (int j = lane; j < groups; j += 32) {
+    const int r = 4 * j;
+    const uint32_t i0 = cid[r];
+    const uint32_t i1 = r + 1 < nc ? cid[r + 1] : i0;
+    const uint32_t i2 = r + 2 < nc ? cid[r + 2] : i0;
+    const uint32_t i3 = r + 3 < nc ? cid[r + 3] : i0;
+    asm volatile(
+        "cp.async.bulk.prefetch.tensor.2d.L2.global.tile::gather4 [%0, {%1, %2, %3, %4, %5}];" ::"l"(
+            rows),
+        "r"(0), "r"(i0), "r"(i1), "r"(i2), "r"(i3)
+        : "memory");
+  }
+}
+
 // Branch-free binary searches over ascending arrays (warp-uniform trip
 // counts, so lanes never diverge).  `top` = largest power of two <= n.
 __device__ __forceinline__ int count_le_bf(const uint32_t *a, int n, int top, uint32_t key) {
@@ -613,6 +634,7 @@ __device__ __forceinline__ bool eval_staged(const GraphView &g, const WarpSmem &
   const int nb = NB > 0 ? NB : (int)g.nb;
   const int A = (int)split_first((uint32_t)nb);
   if (split) prefetch_rows(g, cid, nc, lane);
+  else if (nc > srows && st.rows) prefetch_rows_gather(st.rows, cid + srows, nc - srows, lane);
   else if (nc > srows) prefetch_rows(g, cid + srows, nc - srows, lane);
   const int h = lane & 1, c = lane >> 1;
   for (int p0 = 0; p0 < nc; p0 += srows) {
