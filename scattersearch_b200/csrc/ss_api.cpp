@@ -93,6 +93,7 @@ struct ss_index {
   DevBuf adj;
   uint32_t rstride = 0, max_deg = 0, ep = 0;
   bool has_graph = false;
+  bool row_dups = true;  // some adjacency row repeats an id (found when the graph is set)
 
   std::mutex mu;  // guards err, contexts
   std::string err;
@@ -133,6 +134,7 @@ struct ss_index {
     g.rstride = rstride;
     g.ep = ep;
     g.metric = metric;
+    g.row_dups = row_dups ? 1u : 0u;
     return g;
   }
 };
@@ -466,9 +468,17 @@ int upload_graph(ss_index *h, const std::vector<uint32_t> &adj, uint32_t rstride
   SS_CUDA(h, h->adj.ensure(adj.size() * 4), "adjacency allocation");
   SS_CUDA(h, cudaMemcpy(h->adj.p, adj.data(), adj.size() * 4, cudaMemcpyHostToDevice),
           "adjacency upload");
+  // rows that repeat an id need the kernels' in-row duplicate checks
+  DevBuf flag;
+  SS_CUDA(h, flag.ensure(4, true), "row check allocation");
+  SS_CUDA(h, ssb::launch_row_repeats(h->adj.as<uint32_t>(), h->n, rstride, flag.as<uint32_t>(), 0),
+          "row check");
+  uint32_t dups = 1;
+  SS_CUDA(h, cudaMemcpy(&dups, flag.p, 4, cudaMemcpyDeviceToHost), "row check");
   h->rstride = rstride;
   h->ep = ep;
   h->max_deg = max_deg;
+  h->row_dups = dups != 0;
   h->has_graph = true;
   return SS_OK;
 }

@@ -19,6 +19,7 @@ struct GraphView {
   const uint32_t *adj;   // n x rstride
   uint32_t n, dim, nb, rstride, ep;
   int metric;            // 0 = L2, 1 = inner product
+  uint32_t row_dups;     // 1 = some adjacency row repeats an id (in-row checks needed)
 };
 
 // One batched launch.  Per-query K/L come from Ks/Ls when non-null, else
@@ -85,6 +86,11 @@ SmemPlan plan_intra_smem(const GraphView &g, int L_max, int width, int hash_cap_
 // Launch helpers.  Return cudaSuccess or the launch error.
 //   warps_per_block: teams per CTA; blocks: grid size (0 = one per team
 //   needed for nq with a static schedule).
+// Sets *flag (device word, zeroed by the caller) to 1 when some row of the
+// adjacency (n rows of rstride ids, kNoneId padding) repeats an id.
+cudaError_t launch_row_repeats(const uint32_t *adj, uint32_t n, uint32_t rstride, uint32_t *flag,
+                               cudaStream_t stream);
+
 // Stages whole rows with gather4 copies when p.gather is set and the base
 // rows encode as a tensor map (rows of at most 256 floats, 16-byte aligned
 // base); otherwise with one bulk copy per row.

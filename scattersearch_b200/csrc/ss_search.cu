@@ -986,7 +986,9 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
 #pragma unroll
     for (int c = 0; c < RCH; ++c) {
       const bool valid = row[c] != kNoneId;
-      const unsigned peers = __match_any_sync(kFull, row[c]);
+      // copies of one id in the row: the first in adjacency order counts
+      // (a graph whose rows repeat no id skips the match)
+      const unsigned peers = g.row_dups ? __match_any_sync(kFull, row[c]) : (1u << lane);
       const bool leader = valid && (peers & lanemask_lt) == 0u;
       QProbe pr{};
       // every valid lane probes the table, so the probe overlaps the
@@ -1026,7 +1028,7 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
     //    eviction, a candidate already in the pool (same id under the same
     //    key) is dropped
     const int na = accept_candidates<RCH>(s, nc, size, thr, vis.lossy, lane,
-                                          RCH > 1 && vis.lossy);
+                                          RCH > 1 && vis.lossy && g.row_dups);
     if (na == 0) {
       pref_node = unode;
       if (unode != kNoneId) load_row<RCH>(g, unode, lane, pref_row);
@@ -2303,6 +2305,34 @@ cudaError_t launch_intra_search(const GraphView &g, const BatchArgs &a, const Sm
   if (e != cudaSuccess) return e;
   if (a.nq == 0) return cudaSuccess;
   fn<<<a.nq, width * 32, smem, stream>>>(g, a, p, width);
+  return cudaGetLastError();
+}
+
+namespace {
+// One thread per adjacency row: any id met twice before the padding.
+__global__ void __launch_bounds__(256) row_repeats_kernel(const uint32_t *__restrict__ adj,
+                                                          uint32_t n, uint32_t rstride,
+                                                          uint32_t *flag) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const uint32_t *row = adj + (size_t)r * rstride;
+  for (uint32_t i = 1; i < rstride; ++i) {
+    const uint32_t a = __ldg(row + i);
+    if (a == kNoneId) break;
+    for (uint32_t j = 0; j < i; ++j) {
+      if (__ldg(row + j) == a) {
+        atomicExch(flag, 1u);
+        return;
+      }
+    }
+  }
+}
+}  // namespace
+
+cudaError_t launch_row_repeats(const uint32_t *adj, uint32_t n, uint32_t rstride, uint32_t *flag,
+                               cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  row_repeats_kernel<<<(n + 255) / 256, 256, 0, stream>>>(adj, n, rstride, flag);
   return cudaGetLastError();
 }
 

@@ -240,6 +240,40 @@ def test_repeated_ids_across_row_chunks(oracle_lib):
     idx.close()
 
 
+def test_repeated_ids_within_rows(oracle_lib):
+    """Rows of at most 32 ids (one chunk) where every third row repeats
+    some of its ids: the index notices the repeats when the graph is set and
+    keeps the in-row check, so only the first copy of an id is evaluated
+    (src/annsearch.cpp:229-231); a graph without repeats skips the check
+    and returns the same results for the rows it shares."""
+    O = oracle_lib
+    X, Q, adj0, ep = _synthetic(96 + 5, 6000, 96, 24, 1)
+    rng = np.random.default_rng(17)
+    adj = adj0.copy()
+    for i in range(0, adj.shape[0], 3):
+        d = int((adj[i] != NONE_ID).sum())
+        if d >= 4:
+            k = int(rng.integers(1, 4))
+            src = rng.choice(d, k, replace=False)
+            dst = rng.choice(np.arange(1, d), k, replace=False)
+            adj[i, dst] = adj[i, src]
+    assert adj.shape[1] <= 32
+    assert any(len(set(r[r != NONE_ID].tolist())) < int((r != NONE_ID).sum()) for r in adj)
+    big = _tile(Q)
+    reps = len(big) // len(Q)
+    for graph_adj in (adj, adj0):
+        idx = _index(X, graph_adj, ep, 1)
+        for K, L in ((10, 64), (20, 200)):
+            o_ids, o_d, _, _ = O.search(X, graph_adj, ep, 1, Q, K, L)
+            for tuning in (dict(), dict(hash_cap=512, stage_rows=12)):
+                idx.set_tuning(**tuning)
+                ids, d = idx.search_batch(big, K, L)
+                assert np.array_equal(ids, np.tile(o_ids, (reps, 1))), (K, L, tuning)
+                assert _same_bits(d, np.tile(o_d, (reps, 1))), (K, L, tuning)
+            idx.set_tuning()
+        idx.close()
+
+
 def test_edge_cases(oracle_lib):
     O = oracle_lib
     rng = np.random.default_rng(9)
