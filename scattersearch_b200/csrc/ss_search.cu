@@ -885,67 +885,25 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
   uint32_t ndc = 0, hops = 0;
   int32_t status = kStatusOk;
 
-  // Initial pool: the first min(L, deg(ep)) neighbours of the entry point,
-  // all marked visited, sorted by distance (annsearch.cpp:185-215).  Exact
-  // ties keep adjacency order.
+  // The loop's first pass builds the initial pool: the first min(L, deg(ep))
+  // neighbours of the entry point, all marked visited, sorted by distance
+  // (annsearch.cpp:185-215), exact ties in adjacency order.  It runs as a
+  // hop into an empty pool (every candidate accepted with pool rank 0) from
+  // no slot, except that an id the row repeats enters the pool once per copy,
+  // as the reference's initial pool takes the row as it is.  Each later pass
+  // is one hop.
   int size = 0;
-  {
-    uint32_t row[RCH];
-    load_row<RCH>(g, g.ep, lane, row);
-#pragma unroll
-    for (int c = 0; c < RCH; ++c) {
-      const int m = c * 32 + lane;
-      const bool valid = row[c] != kNoneId && m < L;
-      const unsigned peers = __match_any_sync(kFull, row[c]);
-      const bool leader = valid && (peers & lanemask_lt) == 0u;
-      if (valid) s.cid[m] = row[c];
-      QProbe pr{};
-      const bool found = leader && qh_lookup(vis, row[c], pr);
-      qh_record(vis, pr, row[c], leader && !found, lane);
-      __syncwarp();
-      size += __popc(__ballot_sync(kFull, valid));
-    }
-    __syncwarp();
-    if (!eval_staged<NB, DEEP>(g, s, st, sp, p, s.cid, s.ckey, size, false, lane)) {
-      status = kStatusStageTimeout;
-      size = 0;
-    }
-    ndc += size;
-    // pool = candidates ranked by (key, position): every candidate counts as
-    // accepted with pool rank 0
-#pragma unroll
-    for (int c = 0; c < RCH; ++c) {
-      const int e = c * 32 + lane;
-      if (e < size) {
-        s.ak[e] = s.ckey[e];
-        s.aid[e] = s.cid[e];
-        s.acle[e] = 0u;
-      }
-    }
-    __syncwarp();
-    uint32_t nkey[RCH], nid[RCH];
-    int npos[RCH];
-    accepted_positions<RCH>(s, size, lane, nkey, nid, npos, L);
-#pragma unroll
-    for (int c = 0; c < RCH; ++c) {
-      if (npos[c] < L) {
-        s.pk[npos[c]] = nkey[c];
-        s.pid[npos[c]] = nid[c];
-      }
-    }
-    __syncwarp();
-  }
-
-  uint32_t pref_node = kNoneId;
+  uint32_t pref_node = g.ep;
   uint32_t pref_row[RCH];
-  if (size > 0) {
-    pref_node = s.pid[0];
-    load_row<RCH>(g, pref_node, lane, pref_row);
-  }
+  load_row<RCH>(g, g.ep, lane, pref_row);
 
-  int k = size > 0 ? 0 : -1;  // first unexplored slot
+  bool first = true;
+  int k = 0;  // slot expanded by the hop (none in the first pass)
+#pragma unroll 1
   while (k >= 0) {
-    if (hops >= max_hops) {
+    const bool init = first;  // this pass builds the initial pool
+    first = false;
+    if (!init && hops >= max_hops) {
       status = kStatusHopLimit;
       break;
     }
@@ -960,15 +918,17 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
         break;
       }
     }
-    const uint32_t node = s.pid[k];
-    const uint32_t thr = s.pk[size - 1];
+    const uint32_t node = init ? g.ep : s.pid[k];
+    const uint32_t thr = init ? 0xFFFFFFFFu : s.pk[size - 1];
     const uint32_t unode = u >= 0 ? s.pid[u] : kNoneId;
     __syncwarp();
-    if (lane == 0) {
-      s.pid[k] = node | kExplored;
-      if (unode != kNoneId) prefetch_adj_l2(g, unode);
+    if (!init) {
+      if (lane == 0) {
+        s.pid[k] = node | kExplored;
+        if (unode != kNoneId) prefetch_adj_l2(g, unode);
+      }
+      ++hops;
     }
-    ++hops;
     uint32_t row[RCH];
     if (node == pref_node) {
 #pragma unroll
@@ -977,15 +937,16 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
       load_row<RCH>(g, node, lane, row);
     }
 
-    // 2. in-row dedupe, visited filter, compaction in m order.  The row
-    //    copies of the first stage load start as soon as the fresh ids are
-    //    known; the table is updated while they are in flight.
+    // 2. in-row dedupe, visited filter, compaction in m order (the initial
+    //    pool: the row's first L entries as they are).  The row copies of
+    //    the first stage load start as soon as the fresh ids are known; the
+    //    table is updated while they are in flight.
     int nc = 0;
     const int srows = (int)p.stage_rows;
     bool issued = false;
 #pragma unroll
     for (int c = 0; c < RCH; ++c) {
-      const bool valid = row[c] != kNoneId;
+      const bool valid = row[c] != kNoneId && (!init || c * 32 + lane < L);
       // copies of one id in the row: the first in adjacency order counts
       // (a graph whose rows repeat no id skips the match)
       const unsigned peers = g.row_dups ? __match_any_sync(kFull, row[c]) : (1u << lane);
@@ -994,7 +955,7 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
       // every valid lane probes the table, so the probe overlaps the
       // match above instead of waiting for it; only leaders count
       const bool seen = valid ? qh_lookup(vis, row[c], pr) : true;
-      const bool fresh = leader && !seen;
+      const bool fresh = init ? valid : leader && !seen;
       const unsigned fm = __ballot_sync(kFull, fresh);
       if (fresh) s.cid[nc + __popc(fm & lanemask_lt)] = row[c];
       nc += __popc(fm);
@@ -1006,7 +967,7 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
           issued = true;
         }
       }
-      qh_record(vis, pr, row[c], fresh, lane);
+      qh_record(vis, pr, row[c], leader && !seen, lane);
       __syncwarp();
     }
     if (nc == 0) {
@@ -1027,8 +988,8 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
     // 4. acceptance in adjacency order, with each key's pool rank; after an
     //    eviction, a candidate already in the pool (same id under the same
     //    key) is dropped
-    const int na = accept_candidates<RCH>(s, nc, size, thr, vis.lossy, lane,
-                                          RCH > 1 && vis.lossy && g.row_dups);
+    const int na = accept_candidates<RCH>(s, nc, size, thr, !init && vis.lossy, lane,
+                                          !init && RCH > 1 && vis.lossy && g.row_dups);
     if (na == 0) {
       pref_node = unode;
       if (unode != kNoneId) load_row<RCH>(g, unode, lane, pref_row);
