@@ -295,6 +295,18 @@ int ss_set_stage_layout(ss_index *h, int stage_rows, int stages_per_block);
 enum { SS_ROW_COPY_AUTO = 0, SS_ROW_COPY_BULK = 1 };
 int ss_set_row_copy(ss_index *h, int mode);
 
+/* Visited ids of the batched kernel.  Each query team keeps a small table
+ * in shared memory that may forget ids (a forgotten id met again is
+ * evaluated again: the same results, more bytes read).
+ * SS_VISITED_MARKS_AUTO: persistent batched launches (ss_search_batch*,
+ * plans) also give each team slot one byte per base row in device memory
+ * (n bytes x the launch's team slots, allocated once per search context
+ * when it takes at most a quarter of the free memory and 16 GB), so no id
+ * is evaluated twice.  SS_VISITED_MARKS_OFF: the shared-memory table alone.
+ * Results never depend on it. */
+enum { SS_VISITED_MARKS_AUTO = 0, SS_VISITED_MARKS_OFF = 1 };
+int ss_set_visited_marks(ss_index *h, int mode);
+
 /* ---- exact brute force -------------------------------------------------- */
 
 /* Exact k nearest base rows of each query by brute force (no graph needed);

@@ -62,6 +62,7 @@ SIGNATURES = {
     "ss_set_tuning": (_i32, [_vp, _i32, _i32, _i32]),
     "ss_set_stage_layout": (_i32, [_vp, _i32, _i32]),
     "ss_set_row_copy": (_i32, [_vp, _i32]),
+    "ss_set_visited_marks": (_i32, [_vp, _i32]),
     "ss_search_scatter_batch": (_i32, [_vp, _f32p, _u32, _i32, _i32, _i32, _i32, ctypes.c_uint64,
                                        _u32p, _f32p]),
     "ss_search_scatter_batch_stats": (_i32, [_vp, _f32p, _u32, _i32, _i32, _i32, _i32,

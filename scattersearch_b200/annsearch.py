@@ -378,6 +378,16 @@ class ANNSearch:
         or ROW_COPY_BULK, one bulk copy per row; never changes results."""
         self._check(self._lib.ss_set_row_copy(self._h, int(mode)))
 
+    VISITED_MARKS_AUTO = 0
+    VISITED_MARKS_OFF = 1
+
+    def set_visited_marks(self, mode: int = 0):
+        """Visited ids of the batched kernel (ss_set_visited_marks):
+        VISITED_MARKS_AUTO adds exact per-team marks in device memory to the
+        shared-memory table, VISITED_MARKS_OFF keeps the table alone; never
+        changes results."""
+        self._check(self._lib.ss_set_visited_marks(self._h, int(mode)))
+
 
 class SearchPlan:
     """A graph-captured batched search (ss_plan_*): ``launch(stream)``

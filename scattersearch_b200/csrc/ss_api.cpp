@@ -74,6 +74,7 @@ struct SearchCtx {
   cudaStream_t stream = nullptr;
   DevBuf q, ids, dists, Ks, Ls, off, counter, status, ndc, hops, spill, bf_q, bf_qpack, bf_cand,
       bf_err;
+  DevBuf marks, mark_epoch;  // the warp kernel's per-team visited marks (see visited_marks)
   std::vector<int32_t> h_status;
   ~SearchCtx() {
     if (stream) cudaStreamDestroy(stream);
@@ -123,6 +124,7 @@ struct ss_index {
   int shared_stages = 0;  // row stages shared by a CTA's teams (0 = one per team)
   int stage_rows = 0;     // rows per row stage (0 = 16)
   int row_copy = SS_ROW_COPY_AUTO;  // how row stages are filled (ss_set_row_copy)
+  int visited_marks = SS_VISITED_MARKS_AUTO;  // ss_set_visited_marks
 
   ssb::GraphView view() const {
     ssb::GraphView g;
@@ -351,6 +353,44 @@ int small_hash_cap(int L_max) {
   return (int)slots;
 }
 
+// Bytes of the warp kernel's visited marks per team slot: one per base row,
+// rounded up to 16 (the kernel clears them with 16-byte stores).
+uint32_t mark_stride(const ss_index *h) { return round_up(h->n, 16); }
+
+// Whether `bytes` of new visited marks may be allocated: at most a quarter
+// of the free device memory and 16 GB.
+bool marks_fit(size_t bytes) {
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return false;
+  return bytes <= free_b / 4 && bytes <= (16ull << 30);
+}
+
+// Points a persistent launch of `slots` team slots at the visited marks of
+// context `c`, allocating (or growing) them on first use; leaves a.marks
+// null when they are off or do not fit.  Marks and epochs are cleared
+// together whenever either is reallocated, so no stale mark can equal a new
+// epoch.
+int attach_marks(ss_index *h, SearchCtx *c, size_t slots, ssb::BatchArgs &a,
+                 cudaStream_t stream) {
+  a.marks = nullptr;
+  a.mark_epoch = nullptr;
+  a.mark_stride = 0;
+  if (h->visited_marks != SS_VISITED_MARKS_AUTO || slots == 0) return SS_OK;
+  const size_t mb = slots * mark_stride(h), eb = slots * 4;
+  if (c->marks.cap < mb || c->mark_epoch.cap < eb) {
+    if (!marks_fit(mb > c->marks.cap ? mb - c->marks.cap : 0)) return SS_OK;
+    SS_CUDA(h, c->marks.ensure(mb), "visited marks allocation");
+    SS_CUDA(h, c->mark_epoch.ensure(eb), "visited marks allocation");
+    SS_CUDA(h, cudaMemsetAsync(c->marks.p, 0, c->marks.cap, stream), "visited marks clear");
+    SS_CUDA(h, cudaMemsetAsync(c->mark_epoch.p, 0, c->mark_epoch.cap, stream),
+            "visited marks clear");
+  }
+  a.marks = c->marks.as<uint8_t>();
+  a.mark_epoch = c->mark_epoch.as<uint32_t>();
+  a.mark_stride = mark_stride(h);
+  return SS_OK;
+}
+
 // Core batched launch into caller-provided device buffers on `stream`.
 int launch_batch(ss_index *h, SearchCtx *c, const float *d_q, uint32_t nq, const int32_t *d_K,
                  const int32_t *d_L, const int64_t *d_off, int K0, int L0, int L_max,
@@ -382,7 +422,11 @@ int launch_batch(ss_index *h, SearchCtx *c, const float *d_q, uint32_t nq, const
   a.hops = d_hops;
   a.status = c->status.as<int32_t>();
   a.work_counter = persistent ? c->counter.as<uint32_t>() : nullptr;
-  a.max_hops = h->n + 1;  // the warp kernel's visited table needs no global memory
+  a.max_hops = h->n + 1;
+  if (persistent) {
+    const int rc = attach_marks(h, c, (size_t)blocks * (size_t)wpb, a, stream);
+    if (rc) return rc;
+  }
   if (persistent) SS_CUDA(h, cudaMemsetAsync(c->counter.p, 0, 4, stream), "counter reset");
   SS_CUDA(h, cudaMemsetAsync(c->status.p, 0, (size_t)nq * 4, stream), "status reset");
   SS_CUDA(h, ssb::launch_warp_search(g, a, plan, wpb, blocks, stream), "search launch");
@@ -838,6 +882,7 @@ struct ss_plan {
   uint32_t nq = 0;
   int32_t *status = nullptr;
   uint32_t *counter = nullptr;
+  SearchCtx marks;  // the plan's own visited marks (only marks/mark_epoch are used)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
 };
@@ -912,6 +957,17 @@ int ss_plan_create_uneven(ss_index *h, const float *queries, uint32_t nq, const 
   a.status = p->status;
   a.work_counter = p->counter;
   a.max_hops = h->n + 1;
+  // marks are allocated and cleared before the capture; the graph only
+  // reads and advances them
+  rc = attach_marks(h, &p->marks, (size_t)blocks * (size_t)wpb, a, cs);
+  if (rc == SS_OK) e = cudaStreamSynchronize(cs);
+  if (rc != SS_OK || e != cudaSuccess) {
+    plan_free(p);
+    cudaStreamDestroy(cs);
+    if (rc != SS_OK) return rc;
+    std::lock_guard<std::mutex> lk(h->mu);
+    return cuda_fail(h, e, "plan visited marks");
+  }
   e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
     cudaError_t e1 = cudaMemsetAsync(p->counter, 0, 4, cs);
@@ -1316,6 +1372,14 @@ int ss_set_stage_layout(ss_index *h, int stage_rows, int stages_per_block) {
     return set_err(h, SS_ERR_INVALID_ARGUMENT, "stages_per_block must be in [0, 32]");
   h->stage_rows = stage_rows;
   h->shared_stages = stages_per_block;
+  return SS_OK;
+}
+
+int ss_set_visited_marks(ss_index *h, int mode) {
+  if (!h) return fail(nullptr, SS_ERR_INVALID_ARGUMENT, "null index handle");
+  if (mode != SS_VISITED_MARKS_AUTO && mode != SS_VISITED_MARKS_OFF)
+    return set_err(h, SS_ERR_INVALID_ARGUMENT, "unknown visited marks mode %d", mode);
+  h->visited_marks = mode;
   return SS_OK;
 }
 

@@ -40,6 +40,13 @@ struct BatchArgs {
   uint32_t *spill_bits;    // per-slot visited bitsets, spill_words each
   uint32_t spill_words;
   uint32_t max_hops;
+  // warp kernel: exact visited marks per team slot (blockIdx * teams + team):
+  // one byte per base row holding the epoch of the slot's query that
+  // visited it, mark_stride bytes per slot; mark_epoch[slot] = the slot's
+  // last epoch.  Null = the shared-memory table alone.
+  uint8_t *marks;
+  uint32_t *mark_epoch;
+  uint32_t mark_stride;
 };
 
 // Per-team shared-memory plan (sizes in 4-byte words, all multiples of 4).

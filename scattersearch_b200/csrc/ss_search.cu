@@ -847,6 +847,17 @@ __device__ __forceinline__ void merge_accepted(const WarpSmem &s, int &size, int
   size = min(L, size + na);
 }
 
+// Visited marks of a row's ids (0 for padding), read through L2: byte
+// marks[id] holds the epoch of the team's query that last visited id.  A
+// null `marks` reads nothing.
+template <int RCH>
+__device__ __forceinline__ void load_marks(const uint8_t *marks, const uint32_t (&row)[RCH],
+                                           uint32_t (&mk)[RCH]) {
+#pragma unroll
+  for (int c = 0; c < RCH; ++c)
+    mk[c] = (marks != nullptr && row[c] != kNoneId) ? (uint32_t)__ldcg(marks + row[c]) : 0u;
+}
+
 // One query, one warp.  Each hop (batch-merge form of annsearch.cpp:218-253):
 //   1. expand pool slot k, the first unexplored one (known from the previous
 //      hop); u is the unexplored slot after it;
@@ -859,15 +870,25 @@ __device__ __forceinline__ void merge_accepted(const WarpSmem &s, int &size, int
 //   5. stable-merge the accepted candidates into the pool, older entries
 //      first on ties, truncated to L (InsertIntoPool upper-bound insert,
 //      util.h:56-75; :242-243).
-// After step 4 the next expansion is known (u, unless the best accepted
-// candidate lands before it), so its adjacency row loads during step 5, and
-// u's row is sent to L2 at the start of the hop.
+// After step 4 the next expansion is known: u, unless the best accepted
+// candidate lands before it.  u's adjacency row is loaded at the start of
+// the hop and its visited marks after step 2, so when u is next both are in
+// registers; otherwise the next node's row loads during step 5 and its marks
+// after it.
+//
+// Visited ids: the shared-memory table (QHash) may forget ids, and a
+// forgotten id met again is evaluated again (results unchanged, bytes
+// wasted: 1.4 evaluations per distinct id at 2048 slots and L = 400).  With
+// `marks` (this team's byte per base row, `epoch` = this query's value) an
+// id the table does not hold is looked up there too, so no id is evaluated
+// twice.  The marks of the next row are loaded once it is chosen, so their
+// L2 round trip overlaps the rest of the hop.
 template <int NB, int RCH, bool DEEP>
 __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qsrc, int K, int L,
                                 uint32_t *out_ids, float *out_dists, uint32_t *out_ndc,
                                 uint32_t *out_hops, int32_t *out_status, const WarpSmem &s,
                                 const SmemPlan &p, RowStage &st, const StagePool &sp,
-                                uint32_t max_hops, int lane) {
+                                uint32_t max_hops, uint8_t *marks, uint32_t epoch, int lane) {
   const unsigned lanemask_lt = (1u << lane) - 1u;
   const int qw = (int)g.nb * 8;
   for (int i = lane; i < qw; i += 32) s.q[i] = i < (int)g.dim ? qsrc[i] : 0.f;
@@ -894,8 +915,9 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
   // is one hop.
   int size = 0;
   uint32_t pref_node = g.ep;
-  uint32_t pref_row[RCH];
+  uint32_t pref_row[RCH], pref_mark[RCH];
   load_row<RCH>(g, g.ep, lane, pref_row);
+  load_marks<RCH>(marks, pref_row, pref_mark);
 
   bool first = true;
   int k = 0;  // slot expanded by the hop (none in the first pass)
@@ -923,19 +945,26 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
     const uint32_t unode = u >= 0 ? s.pid[u] : kNoneId;
     __syncwarp();
     if (!init) {
-      if (lane == 0) {
-        s.pid[k] = node | kExplored;
-        if (unode != kNoneId) prefetch_adj_l2(g, unode);
-      }
+      if (lane == 0) s.pid[k] = node | kExplored;
       ++hops;
     }
-    uint32_t row[RCH];
-    if (node == pref_node) {
-#pragma unroll
-      for (int c = 0; c < RCH; ++c) row[c] = pref_row[c];
-    } else {
-      load_row<RCH>(g, node, lane, row);
+    // node's row and marks were loaded when it was chosen (pref_node is
+    // always node; the reload only guards that)
+    if (node != pref_node) {
+      load_row<RCH>(g, node, lane, pref_row);
+      load_marks<RCH>(marks, pref_row, pref_mark);
     }
+    const uint32_t(&row)[RCH] = pref_row;
+    const uint32_t(&rmark)[RCH] = pref_mark;
+    // u is the next node unless an accepted candidate lands before it: its
+    // row loads now, its marks once this hop's marks are stored (below)
+    uint32_t spec_row[RCH], spec_mark[RCH];
+#pragma unroll
+    for (int c = 0; c < RCH; ++c) {
+      spec_row[c] = kNoneId;
+      spec_mark[c] = 0u;
+    }
+    if (unode != kNoneId) load_row<RCH>(g, unode, lane, spec_row);
 
     // 2. in-row dedupe, visited filter, compaction in m order (the initial
     //    pool: the row's first L entries as they are).  The row copies of
@@ -954,7 +983,8 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
       QProbe pr{};
       // every valid lane probes the table, so the probe overlaps the
       // match above instead of waiting for it; only leaders count
-      const bool seen = valid ? qh_lookup(vis, row[c], pr) : true;
+      const bool seen =
+          valid ? (qh_lookup(vis, row[c], pr) || (marks != nullptr && rmark[c] == epoch)) : true;
       const bool fresh = init ? valid : leader && !seen;
       const unsigned fm = __ballot_sync(kFull, fresh);
       if (fresh) s.cid[nc + __popc(fm & lanemask_lt)] = row[c];
@@ -968,11 +998,17 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
         }
       }
       qh_record(vis, pr, row[c], leader && !seen, lane);
+      if (marks != nullptr && leader && !seen) __stcg(marks + row[c], (uint8_t)epoch);
       __syncwarp();
     }
+    if (unode != kNoneId) load_marks<RCH>(marks, spec_row, spec_mark);
     if (nc == 0) {
       pref_node = unode;
-      if (unode != kNoneId) load_row<RCH>(g, unode, lane, pref_row);
+#pragma unroll
+      for (int c = 0; c < RCH; ++c) {
+        pref_row[c] = spec_row[c];
+        pref_mark[c] = spec_mark[c];
+      }
       k = u;
       continue;
     }
@@ -992,7 +1028,11 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
                                           !init && RCH > 1 && vis.lossy && g.row_dups);
     if (na == 0) {
       pref_node = unode;
-      if (unode != kNoneId) load_row<RCH>(g, unode, lane, pref_row);
+#pragma unroll
+      for (int c = 0; c < RCH; ++c) {
+        pref_row[c] = spec_row[c];
+        pref_mark[c] = spec_mark[c];
+      }
       k = u;
       continue;
     }
@@ -1016,12 +1056,21 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
       const uint32_t best = __reduce_min_sync(kFull, cand);  // the one lane holding p0
       const uint32_t nxt = (u >= 0 && u < p0) ? unode : best;
       pref_node = nxt;
-      load_row<RCH>(g, nxt, lane, pref_row);
+      if (nxt == unode) {
+#pragma unroll
+        for (int c = 0; c < RCH; ++c) {
+          pref_row[c] = spec_row[c];
+          pref_mark[c] = spec_mark[c];
+        }
+      } else {
+        load_row<RCH>(g, nxt, lane, pref_row);
+      }
       k = (u >= 0 && u < p0) ? u : p0;
     }
 
     // 5. stable merge into the pool (older entries first on ties)
     merge_accepted<RCH>(s, size, na, p0, L, nkey, nid, npos, lane);
+    if (pref_node != unode) load_marks<RCH>(marks, pref_row, pref_mark);
   }
 
   // Results: slots the pool never filled keep the reference's value-
@@ -1093,10 +1142,28 @@ __global__ void __launch_bounds__(256, 2) warp_search_kernel(GraphView g, BatchA
     if (K < 1 || K > L || L > (int)p.pool_cap) {
       if (lane == 0 && a.status) a.status[q] = kStatusBadArgs;
     } else {
+      // this slot's visited marks: a new epoch per query; when the byte
+      // epoch wraps, the slot's marks are cleared first
+      uint8_t *marks = nullptr;
+      uint32_t epoch = 0;
+      if (a.marks != nullptr) {
+        marks = a.marks + (size_t)slot * a.mark_stride;
+        uint32_t e = 0;
+        if (lane == 0) e = a.mark_epoch[slot] + 1u;
+        e = __shfl_sync(kFull, e, 0);
+        if (e > 255u) {
+          uint4 *m4 = reinterpret_cast<uint4 *>(marks);
+          for (uint32_t i = lane; i < a.mark_stride / 16u; i += 32) __stcg(m4 + i, make_uint4(0, 0, 0, 0));
+          e = 1u;
+        }
+        if (lane == 0) a.mark_epoch[slot] = e;
+        __syncwarp();
+        epoch = e;
+      }
       warp_search_one<NB, RCH, DEEP>(g, a.queries + (size_t)q * a.qstride, K, L, a.ids + off,
                                a.dists ? a.dists + off : nullptr, a.ndc ? a.ndc + q : nullptr,
                                a.hops ? a.hops + q : nullptr, a.status ? a.status + q : nullptr, s,
-                               p, st, sp, a.max_hops, lane);
+                               p, st, sp, a.max_hops, marks, epoch, lane);
       // a stage copy that never completed leaves this team's stage unusable:
       // wait once more (bounded) for it and take no further queries
       if (st.broken) {

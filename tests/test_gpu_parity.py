@@ -164,13 +164,18 @@ def test_visited_spill_to_global_bitset(oracle_lib):
     big = _tile(Q)
     reps = len(big) // len(Q)
     o_big_ids, o_big_d = np.tile(o_ids, (reps, 1)), np.tile(o_d, (reps, 1))
-    idx.set_tuning(warps_per_block=4, hash_cap=512)
-    for _ in range(2):  # second pass checks the bitsets were cleared
+    # with the per-team visited marks (default) and without (the forgetful
+    # table alone)
+    for marks in (idx.VISITED_MARKS_AUTO, idx.VISITED_MARKS_OFF):
+        idx.set_visited_marks(marks)
+        idx.set_tuning(warps_per_block=4, hash_cap=512)
+        for _ in range(2):  # second pass checks the bitsets were cleared
+            ids, d = idx.search_batch(big, 50, 400)
+            assert np.array_equal(ids, o_big_ids) and _same_bits(d, o_big_d), marks
+        idx.set_tuning(warps_per_block=8, hash_cap=512, shared_stages=2)
         ids, d = idx.search_batch(big, 50, 400)
-        assert np.array_equal(ids, o_big_ids) and _same_bits(d, o_big_d)
-    idx.set_tuning(warps_per_block=8, hash_cap=512, shared_stages=2)
-    ids, d = idx.search_batch(big, 50, 400)
-    assert np.array_equal(ids, o_big_ids) and _same_bits(d, o_big_d)
+        assert np.array_equal(ids, o_big_ids) and _same_bits(d, o_big_d), marks
+    idx.set_visited_marks()
     idx.set_tuning(warps_per_block=4, hash_cap=512)
     for W in (1, 4):
         o_w, _, _, _ = O.search(X, adj, ep, 0, Q[:16], 50, 400, W=W)
@@ -219,9 +224,11 @@ def test_repeated_ids_across_row_chunks(oracle_lib):
         o_ids, o_d, ndc, _ = O.search(X, adj, ep, 0, Q, K, L)
         if L == 400:
             assert ndc.max() > 1024  # far more ids than the 512-slot table holds
-        for tuning in (dict(warps_per_block=4, hash_cap=512), dict(hash_cap=512, stage_rows=12),
-                       dict()):
+        for tuning, marks in ((dict(warps_per_block=4, hash_cap=512), 0),
+                              (dict(warps_per_block=4, hash_cap=512), 1),
+                              (dict(hash_cap=512, stage_rows=12), 1), (dict(), 0)):
             idx.set_tuning(**tuning)
+            idx.set_visited_marks(marks)
             ids, d = idx.search_batch(big, K, L)
             assert np.array_equal(ids, np.tile(o_ids, (reps, 1))), (K, L, tuning)
             assert _same_bits(d, np.tile(o_d, (reps, 1))), (K, L, tuning)
@@ -355,6 +362,12 @@ def test_device_api_matches_host_api(oracle_lib):
     # forgot ids only adds distance evaluations
     assert np.array_equal(hops.cpu().numpy().view(np.uint32), o_hops)
     assert (ndc.cpu().numpy().view(np.uint32) >= o_ndc).all()
+    # with the visited marks, a small table evaluates each id once
+    idx.set_tuning(hash_cap=512)
+    idx.search_batch_device(q, nq, ids, d, K=20, L=64, ndc=ndc, hops=hops, stream=s.cuda_stream)
+    s.synchronize()
+    assert np.array_equal(ids.cpu().numpy().view(np.uint32), ids_h)
+    assert np.array_equal(ndc.cpu().numpy().view(np.uint32), o_ndc)
     # with a table large enough never to forget, the counts are the reference's
     idx.set_tuning(hash_cap=65536)
     idx.search_batch_device(q, nq, ids, d, K=20, L=64, ndc=ndc, hops=hops, stream=s.cuda_stream)
@@ -548,4 +561,46 @@ def test_gather_and_bulk_row_copies_agree(oracle_lib, dim, metric):
     # small launches take the latency layout (32-row stages)
     ids, d = idx.search_batch(Q[:20], K, L)
     assert np.array_equal(ids, o_ids[:20]) and _same_bits(d, o_d[:20])
+    idx.close()
+
+
+def test_visited_marks_count_each_id_once_across_epochs(oracle_lib):
+    """Per-team visited marks in device memory: with a 512-slot table that
+    forgets most ids, every query evaluates exactly the reference's distinct
+    ids (the oracle's count), and ids and distance bits stay the oracle's.
+    One team per SM and repeated launches take every team slot through more
+    than 255 queries, so each slot's byte epochs wrap and its marks are
+    cleared on the device; without marks the same table evaluates more."""
+    import torch
+    O = oracle_lib
+    X, Q, adj, ep = _synthetic(11, 20000, 64, 32, 0, clusters=4)
+    idx = _index(X, adj, ep, 0)
+    K, L = 20, 300
+    o_ids, o_d, o_ndc, o_hops = O.search(X, adj, ep, 0, Q, K, L)
+    assert o_ndc.max() > 1024
+    big = _tile(Q, 3000)
+    reps = len(big) // len(Q)
+    t_ids, t_d, t_ndc = np.tile(o_ids, (reps, 1)), np.tile(o_d, (reps, 1)), np.tile(o_ndc, reps)
+    q = torch.as_tensor(big).cuda()
+    nq = q.shape[0]
+    ids = torch.empty((nq, K), dtype=torch.int32, device="cuda")
+    d = torch.empty((nq, K), dtype=torch.float32, device="cuda")
+    ndc = torch.empty(nq, dtype=torch.int32, device="cuda")
+    s = torch.cuda.current_stream()
+    idx.set_tuning(warps_per_block=1, hash_cap=512, blocks_per_sm_cap=1)
+    per_slot = nq / torch.cuda.get_device_properties(0).multi_processor_count
+    launches = int(300 / per_slot) + 2
+    for it in range(launches):
+        idx.search_batch_device(q, nq, ids, d, K=K, L=L, ndc=ndc, stream=s.cuda_stream)
+        s.synchronize()
+        assert idx.batch_status() == 0
+        assert np.array_equal(ids.cpu().numpy().view(np.uint32), t_ids), it
+        assert _same_bits(d.cpu().numpy(), t_d), it
+        assert np.array_equal(ndc.cpu().numpy().view(np.uint32), t_ndc), it
+    idx.set_visited_marks(idx.VISITED_MARKS_OFF)
+    idx.search_batch_device(q, nq, ids, d, K=K, L=L, ndc=ndc, stream=s.cuda_stream)
+    s.synchronize()
+    assert np.array_equal(ids.cpu().numpy().view(np.uint32), t_ids)
+    assert ndc.cpu().numpy().view(np.uint32).sum() > t_ndc.sum()
+    idx.set_tuning()
     idx.close()
