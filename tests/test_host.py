@@ -285,7 +285,7 @@ def test_bench_clock_samples_and_profiled_traffic(tmp_path, monkeypatch):
     c2 = s2.stop()
     assert c2["samples"] == 1 and c2["window"] == "right after the timed steps"
     # the roofline's traffic: the committed small-case bytes per evaluated row,
-    # scaled by the rows a launch evaluates (10k queries x 9,639 rows here)
-    traffic, src = bench.profiled_traffic("cfg3", 10000 * 9639)
+    # scaled by the rows a launch evaluates (10k queries x 6,875 rows here)
+    traffic, src = bench.profiled_traffic("cfg3", 10000 * 6875)
     assert ".md:" in src and 5e10 < traffic < 8e10
-    assert bench.profiled_traffic("cfg2", 10000 * 9639) == (None, None)
+    assert bench.profiled_traffic("cfg2", 10000 * 6875) == (None, None)
