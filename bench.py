@@ -93,6 +93,7 @@ def parse_args(argv=None):
     ap.add_argument("--no-online", action="store_true",
                     help="skip the serving, intra-query and ScatterSearch latency legs")
     ap.add_argument("--no-config1", action="store_true", help="skip the configuration-1 leg")
+    ap.add_argument("--no-config2", action="store_true", help="skip the configuration-2 leg")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the id-parity record against the parity-built reference")
     ap.add_argument("--layout", default=None,
@@ -647,6 +648,114 @@ def measure_config1(device, steps, warmup):
     return out
 
 
+def measure_config2(device, steps, warmup, nq=10000, sample=1000):
+    """Configuration 2 (1M x 128 integer-valued L2 data, NSG-style graph with
+    R <= 64, K = 10, L = 256 -- the largest L the configuration lists --,
+    10,000 queries): the batched search on the device with its roofline
+    fraction, through the C ABI with host buffers, the reference's -Ofast
+    search on the host cores, and, on a 1,000-query sample, id parity with
+    the parity-built reference and recall@10 of both.  Integer coordinates
+    make every distance exact in float32 (so the brute force is exact) and
+    exact ties common."""
+    import torch
+    from oracle import oracle as O
+    from scattersearch_b200 import ANNSearch, datasets, graph
+    t0 = time.time()
+    w = datasets.config(2, n_queries=nq)
+    X = torch.from_numpy(w.base).to(device)
+    adj, ep = graph.build_graph(X, R=w.graph_R, knn_k=w.graph_knn, device=device)
+    Q = torch.from_numpy(w.queries).to(device)
+    torch.cuda.empty_cache()
+    gt, _ = ground_truth(X, Q, w.metric, device)
+    log(f"config 2 setup {time.time() - t0:.1f}s")
+    n, dim = w.base.shape
+    K, L = w.K, max(w.L_list)
+    idx = ANNSearch(dim, n, X, w.metric, base_on_device=True)
+    idx.SetGraph(adj, ep)
+    ids_d = torch.empty((nq, K), dtype=torch.int32, device=device)
+    ndc_d = torch.empty(nq, dtype=torch.int32, device=device)
+    hops_d = torch.empty(nq, dtype=torch.int32, device=device)
+    st = torch.cuda.current_stream()
+    for _ in range(warmup):
+        idx.search_batch_device(Q, nq, ids_d, None, K=K, L=L, stream=st.cuda_stream)
+    torch.cuda.synchronize()
+    evs = []
+    for _ in range(steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        idx.search_batch_device(Q, nq, ids_d, None, K=K, L=L, stream=st.cuda_stream)
+        b.record(st)
+        evs.append((a, b))
+    torch.cuda.synchronize()
+    dev_ms = [a.elapsed_time(b) for a, b in evs]
+    ids = ids_d.cpu().numpy().view(np.uint32)
+    # per-query evaluations and hops (an untimed pass)
+    idx.search_batch_device(Q, nq, ids_d, None, K=K, L=L, ndc=ndc_d, hops=hops_d,
+                            stream=st.cuda_stream)
+    torch.cuda.synchronize()
+    ndc = ndc_d.cpu().numpy().view(np.uint32).astype(np.float64)
+    hops = hops_d.cpu().numpy().view(np.uint32).astype(np.float64)
+    e2e = []
+    for i in range(warmup + steps):
+        t1 = time.perf_counter()
+        h_ids, _ = idx.search_batch(w.queries, K, L)
+        if i >= warmup:
+            e2e.append(time.perf_counter() - t1)
+    rstride = idx.rstride
+    idx.close()
+    del X, Q
+    torch.cuda.empty_cache()
+    mean_s = sum(dev_ms) / len(dev_ms) / 1e3
+    bytes_q = ndc * 4 * dim + hops * 4 * rstride + 4 * dim
+    peak, peak_kind = measured_hbm_peak()
+    out = {"workload": "1Mx128 integer-valued (clipped Gamma), L2, NSG R<=64, K=10, L=256, "
+                       f"{nq} queries, batched persistent",
+           "device_qps": nq / mean_s, "ms_per_batch": 1e3 * mean_s,
+           "e2e_qps": nq * steps / sum(e2e),
+           "ids_equal_e2e_device": bool(np.array_equal(h_ids, ids)),
+           "recall@10_gpu": recall_at_10(ids, gt),
+           "mean_degree": float((adj != 0xFFFFFFFF).sum(1).mean()),
+           "roofline": {"bound": "hbm", "achieved": float(bytes_q.sum()) / mean_s / 1e9,
+                        "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
+                        "frac": float(bytes_q.sum()) / mean_s / 1e9 / peak,
+                        "ndc_per_query": float(ndc.mean()), "hops_per_query": float(hops.mean())}}
+    th = cpu_threads()
+    qs = np.ascontiguousarray(w.queries[:sample])
+    if O.have_reference(fast=True):
+        with stdout_to_stderr():
+            fast = O.RefIndex(w.base, w.metric, adj, ep, fast=True)
+            fast.search(qs, K, L, nthreads=th)
+            reps, t1 = 0, time.perf_counter()
+            while reps < 3 or time.perf_counter() - t1 < 2.0:
+                fast.search(qs, K, L, nthreads=th)
+                reps += 1
+            out["reference_cpu_qps"] = sample * reps / (time.perf_counter() - t1)
+            out["reference_cpu"] = (f"-Ofast SearchArraySimulation, OpenMP over queries, {th} "
+                                    f"threads, first {sample} queries")
+            fast.close()
+            ref = O.RefIndex(w.base, w.metric, adj, ep)
+            r_ids = ref.search(qs, K, L, nthreads=th)
+            ref.close()
+        tie = O.init_ties(w.base, adj, ep, qs, L, w.metric)
+        same = (r_ids == ids[:sample]).all(1)
+        out.update({"parity_reference": "oracle/_ref/libssref.so (parity build)",
+                    "parity_sample": sample, "init_tie_queries": int(tie.sum()),
+                    "ids_equal_fraction": float(same.mean()),
+                    "ids_equal_fraction_excluding_init_ties": float(same[~tie].mean())
+                    if (~tie).any() else None,
+                    "recall@10_gpu_sample": recall_at_10(ids[:sample], gt),
+                    "recall@10_reference_sample": recall_at_10(r_ids, gt)})
+    # the reference algorithm's evaluation count on the sample (the oracle's
+    # exact visited set) against the device's
+    _, _, o_ndc, o_hops = O.search(w.base, adj, ep, w.metric, qs, K, L)
+    out["device_evals_equal_reference_count"] = bool(
+        np.array_equal(ndc[:sample].astype(np.uint32), np.asarray(o_ndc, np.uint32)))
+    out["hops_equal_reference"] = bool(
+        np.array_equal(hops[:sample].astype(np.uint32), np.asarray(o_hops, np.uint32)))
+    log("config 2: " + ", ".join(f"{k} {v}" for k, v in out.items() if k != "workload"))
+    return out
+
+
 def measure_scatter_reference(idx, wl, device, nq=300, widths=(4, 8)):
     """ScatterSearch's intra-query search, one query at a time, next to the
     reference's own on the same queries (the tests/parallel_search.cpp:76-95
@@ -901,11 +1010,17 @@ def run_ours(args):
     parity = parity_record(wl, ids_np, L) if solo and not args.no_parity else None
     online = measure_online(idx, wl) if solo and not args.no_online else None
     intra = measure_intra_latency(idx, wl, L, device) if solo and not args.no_online else None
-    scatter = measure_scatter_reference(idx, wl, device) if solo and not args.no_online else None
+    # the reference's ScatterSearch starts its election from best_dist = 1000
+    # (src/annsearch.cpp:850), which large L2 distances break (recall near 0,
+    # and a host crash on configuration 2's data): inner-product workloads only
+    scatter = measure_scatter_reference(idx, wl, device) \
+        if solo and not args.no_online and wl["metric"] == 1 else None
     idx.set_tuning(tune["warps_per_block"], tune["hash_cap"], 0, tune["shared_stages"],
                    tune["stage_rows"])
     config1 = measure_config1(device, args.steps, args.warmup) \
         if solo and not args.no_config1 and args.workload == "cfg3" and args.scale == 1.0 else None
+    config2 = measure_config2(device, args.steps, args.warmup) \
+        if solo and not args.no_config2 and args.workload == "cfg3" and args.scale == 1.0 else None
 
     peak, peak_kind = measured_hbm_peak()
     traffic, traffic_src = profiled_traffic(args.workload, ndc_dev.sum()) \
@@ -949,6 +1064,7 @@ def run_ours(args):
         "intra_latency": intra,
         "scatter_vs_reference": scatter,
         "config1": config1,
+        "config2": config2,
         "gpu_launches": args.steps,
         "launch": "one CUDA graph per step (queue reset, status reset, search kernel)",
         "clocks": clocks,
