@@ -163,9 +163,23 @@ __device__ __forceinline__ bool visited_test(const Visited &v, uint32_t id) {
 // check runs only after the first eviction of a query (`lossy`).
 struct QHash {
   uint4 *bkt;
+  uint32_t *evb;  // bit per bucket: the bucket has evicted an id this query
   uint32_t rbits, rmask, bmask;
   bool lossy;  // an id was evicted (or not recorded) during this query
 };
+
+// Words of the per-bucket eviction bits of a table of 2^bbits buckets.
+__host__ __device__ __forceinline__ uint32_t evict_words(uint32_t bbits) {
+  return bbits >= 5 ? (1u << (bbits - 5)) : 1u;
+}
+
+// True when a bucket of the probe has evicted an id this query: only then
+// can an id the table does not hold have been visited.  An id is recorded
+// in one of its two buckets (into an empty slot, or over an evicted one,
+// which sets that bucket's bit), and leaves the table only by eviction.
+__device__ __forceinline__ bool probe_lossy(const QHash &h, uint32_t b1, uint32_t b2) {
+  return ((h.evb[b1 >> 5] >> (b1 & 31u)) | (h.evb[b2 >> 5] >> (b2 & 31u))) & 1u;
+}
 
 constexpr uint32_t kMix1 = 0x9E3779B1u;
 constexpr uint32_t kMix2 = 0x7FEB352Du;
@@ -259,6 +273,7 @@ __device__ __forceinline__ void qh_record(QHash &h, const QProbe &pr, uint32_t i
     } else {
       sl = (id * kMix3) >> 29;
       ev = true;
+      atomicOr(h.evb + (b >> 5), 1u << (b & 31u));
     }
     slots[b * 8 + sl] = (unsigned short)t;
   }
@@ -328,6 +343,7 @@ struct WarpSmem {
   uint32_t *cid, *ckey;            // this hop's fresh candidates, adjacency order
   uint32_t *ak, *aid, *acle;       // accepted candidates (key, id, pool rank), adjacency order
   uint4 *bkt;                      // visited hash buckets
+  uint32_t *evb;                   // per-bucket eviction bits (evict_words)
 };
 
 __device__ __forceinline__ WarpSmem carve_warp(uint32_t *base, const SmemPlan &p) {
@@ -354,6 +370,7 @@ __device__ __forceinline__ WarpSmem carve_warp(uint32_t *base, const SmemPlan &p
     base += p.cand_cap;
   }
   s.bkt = reinterpret_cast<uint4 *>(base);
+  s.evb = base + (1u << p.hash_log2) * 4;
   return s;
 }
 
@@ -858,6 +875,15 @@ __device__ __forceinline__ void load_marks(const uint8_t *marks, const uint32_t 
     mk[c] = (marks != nullptr && row[c] != kNoneId) ? (uint32_t)__ldcg(marks + row[c]) : 0u;
 }
 
+// The marks to read for the next row: none while the table has forgotten
+// nothing this query (every id it does not hold is then fresh), unless rows
+// span several 32-id chunks (a chunk's records may evict an id that a later
+// chunk of the same row repeats).
+template <int RCH>
+__device__ __forceinline__ const uint8_t *mark_src(const uint8_t *marks, const QHash &vis) {
+  return (RCH > 1 || vis.lossy) ? marks : nullptr;
+}
+
 // One query, one warp.  Each hop (batch-merge form of annsearch.cpp:218-253):
 //   1. expand pool slot k, the first unexplored one (known from the previous
 //      hop); u is the unexplored slot after it;
@@ -894,10 +920,12 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
   for (int i = lane; i < qw; i += 32) s.q[i] = i < (int)g.dim ? qsrc[i] : 0.f;
   const uint32_t nbk = 1u << p.hash_log2;
   for (uint32_t i = lane; i < nbk; i += 32) s.bkt[i] = make_uint4(~0u, ~0u, ~0u, ~0u);
+  for (uint32_t i = lane; i < evict_words(p.hash_log2); i += 32) s.evb[i] = 0u;
   __syncwarp();
 
   QHash vis;
   vis.bkt = s.bkt;
+  vis.evb = s.evb;
   vis.rbits = p.qh_rbits;
   vis.rmask = (1u << p.qh_rbits) - 1u;
   vis.bmask = (p.hash_log2 + p.qh_rbits >= 32) ? ~0u : ((1u << (p.hash_log2 + p.qh_rbits)) - 1u);
@@ -917,7 +945,7 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
   uint32_t pref_node = g.ep;
   uint32_t pref_row[RCH], pref_mark[RCH];
   load_row<RCH>(g, g.ep, lane, pref_row);
-  load_marks<RCH>(marks, pref_row, pref_mark);
+  load_marks<RCH>(mark_src<RCH>(marks, vis), pref_row, pref_mark);
 
   bool first = true;
   int k = 0;  // slot expanded by the hop (none in the first pass)
@@ -952,7 +980,7 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
     // always node; the reload only guards that)
     if (node != pref_node) {
       load_row<RCH>(g, node, lane, pref_row);
-      load_marks<RCH>(marks, pref_row, pref_mark);
+      load_marks<RCH>(mark_src<RCH>(marks, vis), pref_row, pref_mark);
     }
     const uint32_t(&row)[RCH] = pref_row;
     const uint32_t(&rmark)[RCH] = pref_mark;
@@ -983,8 +1011,13 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
       QProbe pr{};
       // every valid lane probes the table, so the probe overlaps the
       // match above instead of waiting for it; only leaders count
-      const bool seen =
-          valid ? (qh_lookup(vis, row[c], pr) || (marks != nullptr && rmark[c] == epoch)) : true;
+      bool seen = valid ? qh_lookup(vis, row[c], pr) : true;
+      // the marks are read only where a bucket of the id has evicted, and
+      // the warp waits for them only when some lane needs them
+      if (marks != nullptr) {
+        const bool need = !seen && probe_lossy(vis, pr.b1, pr.b2);
+        if (__any_sync(kFull, need)) seen = seen || (need && rmark[c] == epoch);
+      }
       const bool fresh = init ? valid : leader && !seen;
       const unsigned fm = __ballot_sync(kFull, fresh);
       if (fresh) s.cid[nc + __popc(fm & lanemask_lt)] = row[c];
@@ -1001,7 +1034,7 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
       if (marks != nullptr && leader && !seen) __stcg(marks + row[c], (uint8_t)epoch);
       __syncwarp();
     }
-    if (unode != kNoneId) load_marks<RCH>(marks, spec_row, spec_mark);
+    if (unode != kNoneId) load_marks<RCH>(mark_src<RCH>(marks, vis), spec_row, spec_mark);
     if (nc == 0) {
       pref_node = unode;
 #pragma unroll
@@ -1070,7 +1103,7 @@ __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qs
 
     // 5. stable merge into the pool (older entries first on ties)
     merge_accepted<RCH>(s, size, na, p0, L, nkey, nid, npos, lane);
-    if (pref_node != unode) load_marks<RCH>(marks, pref_row, pref_mark);
+    if (pref_node != unode) load_marks<RCH>(mark_src<RCH>(marks, vis), pref_row, pref_mark);
   }
 
   // Results: slots the pool never filled keep the reference's value-
@@ -2161,13 +2194,14 @@ SmemPlan plan_warp_smem(const GraphView &g, int L_max, int hash_cap_override, in
   // tensor-map box) and a stage of a multiple of 4 rows
   p.gather = (p.stage_split == 1 && g.nb * 8u <= 256u && p.stage_rows % 4u == 0u) ? 1u : 0u;
   p.words_per_team = p.stage_words + 4 + p.q_words + 2 * p.pool_cap + 5 * p.cand_cap +
-                     (1u << bbits) * 4;
+                     (1u << bbits) * 4 + evict_words(bbits);
   p.words_per_team = round_up(p.words_per_team, 32);  // 128-byte aligned stages
   return p;
 }
 
 void share_stages(SmemPlan &p, int stages) {
-  const uint32_t rest = p.q_words + 2 * p.pool_cap + 5 * p.cand_cap + (1u << p.hash_log2) * 4;
+  const uint32_t rest = p.q_words + 2 * p.pool_cap + 5 * p.cand_cap + (1u << p.hash_log2) * 4 +
+                        evict_words(p.hash_log2);
   if (stages > 0) {
     p.shared_stages = (uint32_t)std::min(stages, 32);
     p.words_per_team = round_up(rest, 32);
