@@ -1962,6 +1962,19 @@ __global__ void __launch_bounds__(512) scatter_search_kernel(GraphView g, BatchA
         status = kStatusHopLimit;
         break;
       }
+      // the next unexplored slot's adjacency row is likely the next hop's:
+      // send it to L2 now
+      for (int b0 = k + 1; b0 < size; b0 += 32) {
+        const int idx = b0 + lane;
+        const bool un = idx < size && !(s.pid[idx] & kExplored);
+        const unsigned bm = __ballot_sync(kFull, un);
+        if (bm) {
+          const int u = b0 + __ffs(bm) - 1;
+          const uint32_t unode = s.pid[u] & ~kExplored;
+          if (lane == 0) prefetch_adj_l2(g, unode);
+          break;
+        }
+      }
       // A stealing warp may mark slot k explored after the ballot above (the
       // entry is then its to expand), so the slot is read once, by lane 0,
       // and skipped when taken; the node id never carries the explored bit.
@@ -1992,6 +2005,10 @@ __global__ void __launch_bounds__(512) scatter_search_kernel(GraphView g, BatchA
       }
       if (nc == 0) continue;
       __syncwarp();
+      // the candidate rows go to L2 first: the distance loads read each row
+      // in groups of 8 blocks, and the groups after the first (and the
+      // second 16-row pass) then find their lines there
+      prefetch_rows(g, s.cid, nc, lane);
       eval_candidates<NB>(g, qs, s.cid, s.ckey, nc, lane);
       ndc += nc;
       __syncwarp();
