@@ -679,6 +679,9 @@ __device__ __forceinline__ bool eval_staged(const GraphView &g, const WarpSmem &
       if (p0 > 0 || !first_issued) stage_issue(g, s, st, cid + p0, m, 2, p.stage_row_words, lane);
       if (!stage_wait(st)) return false;
       staged_accumulate<NB, true>(g, s.q, row, h, 0, nb, a0, a1, a2, a3);
+      // the last pass's rows are read: a shared stage goes back before the
+      // lane-pair sums (stage_release waits for every lane's reads)
+      if (p0 + srows >= nc) stage_release(st, sp, lane);
     } else {
       if (p0 > 0 || !first_issued) stage_issue(g, s, st, cid + p0, m, 0, p.stage_row_words, lane);
       if (!stage_wait(st)) return false;
