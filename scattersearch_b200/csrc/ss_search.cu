@@ -19,7 +19,8 @@
 //                        the tensor-memory-access engine: four rows per
 //                        gather4 copy when a row has at most 256 floats, one
 //                        bulk copy per row otherwise; the stage is a team's
-//                        own, or one taken from a pool the CTA's teams share.  Stages deeper than 16
+//                        own, or one taken from a pool the CTA's teams
+//                        share.  Stages deeper than 16
 //                        rows (one copy round trip per hop) are a separate
 //                        instantiation (DEEP), used for launches small
 //                        enough to keep every query resident.
@@ -401,7 +402,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
 // 256 floats), one cp.async.bulk.tensor ... tile::gather4 copies four rows,
 // named by their indices, into four consecutive stage rows; otherwise one
 // cp.async.bulk copies each row.  Issuing a copy costs the team's warp about
-// 60 cycles per instruction, so four rows per instruction cut the issue
+// 60-110 cycles per instruction, so four rows per instruction cut the issue
 // time of a 12-row pass from about 760 to 320 cycles (measured, 8 teams per
 // SM).
 struct RowStage {
@@ -910,8 +911,9 @@ __device__ __forceinline__ const uint8_t *mark_src(const uint8_t *marks, const Q
 // wasted: 1.4 evaluations per distinct id at 2048 slots and L = 400).  With
 // `marks` (this team's byte per base row, `epoch` = this query's value) an
 // id the table does not hold is looked up there too, so no id is evaluated
-// twice.  The marks of the next row are loaded once it is chosen, so their
-// L2 round trip overlaps the rest of the hop.
+// twice.  The next row's marks are loaded as soon as the next node is known
+// (u's during the hop), so their memory round trip overlaps other work, and
+// they are read only for ids whose buckets have evicted (probe_lossy).
 template <int NB, int RCH, bool DEEP>
 __device__ void warp_search_one(const GraphView &g, const float *__restrict__ qsrc, int K, int L,
                                 uint32_t *out_ids, float *out_dists, uint32_t *out_ndc,
