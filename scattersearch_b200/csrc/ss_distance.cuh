@@ -94,12 +94,17 @@ __device__ __forceinline__ float pair_distance(const GraphView &g, const float *
       for (int t = 0; t < NB; ++t) acc_ip(a0, a1, a2, a3, q4[2 * block_at(t, NB)], v[t]);
     }
   } else {
+    // groups of 8 blocks, double-buffered: the next group's loads are in
+    // flight while this group accumulates (same order of operations)
+    float4 v[8], w[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      v[u] = (act && u < nb) ? ldg_f4(row + 2 * block_at(u, nb)) : make_float4(0.f, 0.f, 0.f, 0.f);
     for (int t0 = 0; t0 < nb; t0 += 8) {
-      float4 v[8];
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
-        const int t = t0 + u;
-        v[u] = (act && t < nb) ? ldg_f4(row + 2 * block_at(t, nb)) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const int t = t0 + 8 + u;
+        w[u] = (act && t < nb) ? ldg_f4(row + 2 * block_at(t, nb)) : make_float4(0.f, 0.f, 0.f, 0.f);
       }
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
@@ -109,6 +114,8 @@ __device__ __forceinline__ float pair_distance(const GraphView &g, const float *
           else acc_ip(a0, a1, a2, a3, q4[2 * block_at(t, nb)], v[u]);
         }
       }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) v[u] = w[u];
     }
   }
   // Horizontal sum u0 + u1 + ... + u7, left to right (distance.cpp:53).
