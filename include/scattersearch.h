@@ -148,8 +148,11 @@ int ss_search_batch_device(ss_index *h, const float *queries, uint32_t nq, const
  * L; queries, ids and dists are fixed device buffers; dists may be NULL) --
  * the work-queue reset, the status reset and the persistent search kernel --
  * into a CUDA graph; ss_plan_launch replays it on `stream` with one graph
- * launch.  The plan owns its status words: ss_plan_status reports the failed
- * queries of its last synchronised replay.  Buffers must stay valid while
+ * launch.  The plan owns its status words, work-queue head and visited
+ * marks (ss_set_visited_marks; allocated and cleared at creation):
+ * ss_plan_status reports the failed queries of its last synchronised
+ * replay, and replays of one plan must not overlap on the GPU (order them
+ * on one stream, or use one plan per stream).  Buffers must stay valid while
  * the plan exists; rewrite the query buffer between replays to search new
  * queries. */
 typedef struct ss_plan ss_plan;
