@@ -19,6 +19,12 @@ query) is timed on a sample beside it.  `cpu_baseline` is the reference's
 own SearchArraySimulation (compiled from its sources, -Ofast) on the host
 cores over a bounded sample.
 
+At N = 1 the default line also carries records of configurations 1, 2 and 4
+(`config1`, `config2`, `config4`: device and end-to-end QPS, recall, and
+parity with the parity-built reference or the host baseline; configurations
+2 and 4 with their roofline fraction), each built and measured after the
+headline's timed region; `--no-config1/2/4` skip them.
+
 --impl reference times that reference CPU search alone as the reference arm
 (same workload; rank 0 only under torchrun).
 
@@ -94,6 +100,7 @@ def parse_args(argv=None):
                     help="skip the serving, intra-query and ScatterSearch latency legs")
     ap.add_argument("--no-config1", action="store_true", help="skip the configuration-1 leg")
     ap.add_argument("--no-config2", action="store_true", help="skip the configuration-2 leg")
+    ap.add_argument("--no-config4", action="store_true", help="skip the configuration-4 leg")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the id-parity record against the parity-built reference")
     ap.add_argument("--layout", default=None,
@@ -756,6 +763,37 @@ def measure_config2(device, steps, warmup, nq=10000, sample=1000):
     return out
 
 
+def measure_config4(args, d, device, cpu_seconds=5.0):
+    """Configuration 4 (5M x 96 unit vectors, inner product, NSG-style graph
+    with R <= 32, one batch of 100k queries with per-query K in {1, 10, 100}
+    and L uniform in [32, 512]) as a record of the default run: the same
+    measurement as --workload cfg4 (one graph-captured persistent launch per
+    step, the C-ABI call with host buffers, the plain path on a sample, the
+    oracle's restatement on the host cores for a shorter sample)."""
+    import torch
+    a = argparse.Namespace(**vars(args))
+    a.workload, a.nq, a.scale = "cfg4", 100_000, 1.0
+    t0 = time.time()
+    wl = build_workload(a, 0, 1, device)
+    log(f"config 4 setup {time.time() - t0:.1f}s")
+    rec = uneven_record(a, wl, d, device, cpu_seconds)
+    del wl
+    torch.cuda.empty_cache()
+    out = {"workload": rec["config"]["workload"], "device_qps": rec["value"],
+           "ms_per_batch": rec["ms_per_step"], "e2e_qps": rec["e2e"]["value"],
+           "ids_equal_e2e_device": rec["e2e"]["ids_equal_device_path"],
+           "recall@10_K>=10": rec["config"]["recall@10_K>=10"],
+           "recall@1_K=1": rec["config"]["recall@1_K=1"],
+           "recall_sample": rec["config"]["recall_sample"],
+           "L_mean": rec["config"]["L_mean"], "K_counts": rec["config"]["K_counts"],
+           "tuning": rec["config"]["tuning"], "plain_gpu": rec["plain_gpu"],
+           "roofline": rec["roofline"], "clocks": rec["clocks"]}
+    if "cpu_baseline" in rec:
+        out["cpu_baseline"] = rec["cpu_baseline"]
+    log("config 4: " + ", ".join(f"{k} {v}" for k, v in out.items() if k != "workload"))
+    return out
+
+
 def measure_scatter_reference(idx, wl, device, nq=300, widths=(4, 8)):
     """ScatterSearch's intra-query search, one query at a time, next to the
     reference's own on the same queries (the tests/parallel_search.cpp:76-95
@@ -1021,6 +1059,8 @@ def run_ours(args):
         if solo and not args.no_config1 and args.workload == "cfg3" and args.scale == 1.0 else None
     config2 = measure_config2(device, args.steps, args.warmup) \
         if solo and not args.no_config2 and args.workload == "cfg3" and args.scale == 1.0 else None
+    config4 = measure_config4(args, d, device) \
+        if solo and not args.no_config4 and args.workload == "cfg3" and args.scale == 1.0 else None
 
     peak, peak_kind = measured_hbm_peak()
     traffic, traffic_src = profiled_traffic(args.workload, ndc_dev.sum()) \
@@ -1065,6 +1105,7 @@ def run_ours(args):
         "scatter_vs_reference": scatter,
         "config1": config1,
         "config2": config2,
+        "config4": config4,
         "gpu_launches": args.steps,
         "launch": "one CUDA graph per step (queue reset, status reset, search kernel)",
         "clocks": clocks,
@@ -1111,8 +1152,22 @@ def run_uneven(args):
     d = Dist("nccl")
     torch.cuda.set_device(d.local_rank)
     device = torch.device("cuda", d.local_rank)
-    from scattersearch_b200 import ANNSearch, autotune, datasets
     wl = build_workload(args, d.rank, d.world, device)
+    out = uneven_record(args, wl, d, device, args.cpu_seconds)
+    if d.rank == 0:
+        print(json.dumps(out))
+    d.close()
+    return 0
+
+
+def uneven_record(args, wl, d, device, cpu_seconds):
+    """Measures one built configuration-4 workload: autotuned layout, exact
+    and device evaluation counts, graph-captured replays timed with CUDA
+    events, the C-ABI call with pinned host buffers, the plain per-query path
+    on a sample and (rank 0 of a 1-GPU run) the oracle's restatement on the
+    host cores.  Returns the bench record."""
+    import torch
+    from scattersearch_b200 import ANNSearch, autotune, datasets
     nq, dim = wl["queries"].shape
     Ks, Ls = datasets.uneven_k_l(nq * d.world)
     Ks = np.ascontiguousarray(Ks[d.rank * nq:(d.rank + 1) * nq])
@@ -1254,13 +1309,10 @@ def run_uneven(args):
         "clocks": clocks,
     }
     if d.rank == 0 and d.world == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = time_port_uneven(wl, Ks, Ls, off, ids_np, args.cpu_seconds)
+        out["cpu_baseline"] = time_port_uneven(wl, Ks, Ls, off, ids_np, cpu_seconds)
     plan.close()
     idx.close()
-    if d.rank == 0:
-        print(json.dumps(out))
-    d.close()
-    return 0
+    return out
 
 
 def time_port_uneven(wl, Ks, Ls, off, ids_np, seconds):
