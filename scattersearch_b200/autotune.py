@@ -6,9 +6,13 @@ results: how many query teams share a CTA (``warps_per_block``), how many row
 stages those teams share (``shared_stages``; 0 = one per team, fewer stages
 than teams leave room for more teams per SM) and the size of each query's
 shared-memory visited table (``hash_cap``; a smaller table fits more teams
-per SM but forgets more visited ids, which are then evaluated again).  ``autotune`` times candidate pairs on a sample of the caller's
-queries with CUDA events, checks that every candidate returns the same ids,
-and keeps the fastest.  Choices are cached per (GPU name, dim, adjacency row
+per SM but forgets more visited ids, which are then evaluated again).  A
+fourth choice, the visited marks in device memory behind that table
+(``visited_marks``), stops those repeats at the cost of a mark read where a
+bucket has evicted: at 1.2M x 200 they are worth 5% at L = 400 and cost 12%
+at L = 200, so they are timed too.  ``autotune`` times the candidates on a
+sample of the caller's queries with CUDA events, checks that every candidate
+returns the same ids, and keeps the fastest.  Choices are cached per (GPU name, dim, adjacency row
 stride, L rounded up to a power of two) in a JSON file, so ``apply`` can
 reuse them without timing.
 """
@@ -28,6 +32,8 @@ SHARED_CANDIDATES = ((2, 1), (4, 2), (4, 3), (8, 3), (8, 4), (8, 5))
 # rows per row stage tried with one stage per team (16 = the default; 24 takes
 # most hops' fresh rows in one copy round trip, at fewer teams per SM)
 STAGE_ROWS_CANDIDATES = (16, 12, 24)
+# the fastest layouts with visited marks are timed again without them
+MARKS_OFF_TOP = 6
 _lock = threading.Lock()
 
 
@@ -88,17 +94,19 @@ def apply(index, L: int, path: str = DEFAULT_CACHE, device=None) -> dict | None:
     if choice:
         index.set_tuning(int(choice["warps_per_block"]), int(choice["hash_cap"]), 0,
                          int(choice.get("shared_stages", 0)), int(choice.get("stage_rows", 0)))
+        index.set_visited_marks(int(choice.get("visited_marks", 0)))
     return choice
 
 
 def autotune(index, queries, K: int, L: int, reps: int = 3, path: str | None = DEFAULT_CACHE,
              device=None, wpb_candidates=WPB_CANDIDATES, hash_caps=None, Ks=None, Ls=None,
              out_off=None, shared_candidates=SHARED_CANDIDATES,
-             stage_rows_candidates=STAGE_ROWS_CANDIDATES) -> dict:
+             stage_rows_candidates=STAGE_ROWS_CANDIDATES, marks_off_top=MARKS_OFF_TOP) -> dict:
     """Times every (warps_per_block, shared_stages, stage_rows, hash_cap)
     candidate -- each of ``wpb_candidates`` with a stage per team of each of
     ``stage_rows_candidates`` rows, and each pair of ``shared_candidates``
-    with 16-row stages -- on ``queries`` (a
+    with 16-row stages -- with visited marks, then the ``marks_off_top``
+    fastest of them without (``visited_marks`` 1), on ``queries`` (a
     CUDA tensor, nq x dim) and sets the fastest on ``index``.  Raises if two
     candidates return different ids.  Returns the choice with the timing
     table; stores it in the cache at ``path`` (None: no cache).
@@ -123,35 +131,46 @@ def autotune(index, queries, K: int, L: int, reps: int = 3, path: str | None = D
 
     ref = None
     table = []
+
+    def time_one(wpb, stages, rows, hc, marks):
+        nonlocal ref
+        index.set_tuning(wpb, hc, 0, stages, rows)
+        index.set_visited_marks(marks)
+        launch()
+        stream.synchronize()
+        got = ids.cpu().numpy()
+        if ref is None:
+            ref = got.copy()
+        elif not np.array_equal(got, ref):
+            raise RuntimeError(f"ids differ under warps_per_block={wpb}, "
+                               f"shared_stages={stages}, stage_rows={rows}, hash_cap={hc}, "
+                               f"visited_marks={marks}")
+        times = []
+        for _ in range(reps):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            launch()
+            b.record(stream)
+            stream.synchronize()
+            times.append(a.elapsed_time(b))
+        table.append({"warps_per_block": wpb, "shared_stages": stages, "stage_rows": rows,
+                      "hash_cap": hc, "visited_marks": marks, "ms": float(np.median(times))})
+
     layouts = [(w, 0, r) for r in (stage_rows_candidates or (16,)) for w in wpb_candidates]
     layouts += [(w, st, 16) for w, st in (shared_candidates or ())]
     for hc in (hash_caps or hash_candidates(L)):
         for wpb, stages, rows in layouts:
-            index.set_tuning(wpb, hc, 0, stages, rows)
-            launch()
-            stream.synchronize()
-            got = ids.cpu().numpy()
-            if ref is None:
-                ref = got.copy()
-            elif not np.array_equal(got, ref):
-                raise RuntimeError(f"ids differ under warps_per_block={wpb}, "
-                                   f"shared_stages={stages}, stage_rows={rows}, hash_cap={hc}")
-            times = []
-            for _ in range(reps):
-                a = torch.cuda.Event(enable_timing=True)
-                b = torch.cuda.Event(enable_timing=True)
-                a.record(stream)
-                launch()
-                b.record(stream)
-                stream.synchronize()
-                times.append(a.elapsed_time(b))
-            table.append({"warps_per_block": wpb, "shared_stages": stages, "stage_rows": rows,
-                          "hash_cap": hc, "ms": float(np.median(times))})
+            time_one(wpb, stages, rows, hc, 0)
+    for r in sorted(table, key=lambda r: r["ms"])[:max(0, marks_off_top)]:
+        time_one(r["warps_per_block"], r["shared_stages"], r["stage_rows"], r["hash_cap"], 1)
     best = min(table, key=lambda r: r["ms"])
     index.set_tuning(best["warps_per_block"], best["hash_cap"], 0, best["shared_stages"],
                      best["stage_rows"])
+    index.set_visited_marks(best["visited_marks"])
     choice = {"warps_per_block": best["warps_per_block"], "shared_stages": best["shared_stages"],
-              "stage_rows": best["stage_rows"], "hash_cap": best["hash_cap"], "ms": best["ms"],
+              "stage_rows": best["stage_rows"], "hash_cap": best["hash_cap"],
+              "visited_marks": best["visited_marks"], "ms": best["ms"],
               "sample_queries": nq, "K": "per query" if uneven else K, "L": L}
     if path:
         save_choice(tuning_key(_gpu_name(device if device is not None else dev),

@@ -462,12 +462,20 @@ def test_autotuner_keeps_results_and_caches_its_choice(oracle_lib, tmp_path):
     path = str(tmp_path / "tuning.json")
     choice = autotune.autotune(idx, q, 10, 100, reps=1, path=path)
     assert choice["warps_per_block"] in (1, 2, 4, 8) and choice["hash_cap"] >= 1024
-    assert len(choice["table"]) == (4 * len(autotune.STAGE_ROWS_CANDIDATES) + len(
+    assert choice["visited_marks"] in (0, 1)
+    n_layouts = (4 * len(autotune.STAGE_ROWS_CANDIDATES) + len(
         autotune.SHARED_CANDIDATES)) * len(autotune.hash_candidates(100))
+    # every layout with visited marks, the fastest few again without
+    assert len(choice["table"]) == n_layouts + min(autotune.MARKS_OFF_TOP, n_layouts)
+    assert sum(r["visited_marks"] for r in choice["table"]) == min(autotune.MARKS_OFF_TOP,
+                                                                   n_layouts)
     after, _ = idx.search_batch(fx["queries"], 10, 100)
     assert np.array_equal(before, after)
     idx.set_tuning()
+    idx.set_visited_marks()
     assert autotune.apply(idx, 100, path=path)["hash_cap"] == choice["hash_cap"]
+    again, _ = idx.search_batch(fx["queries"], 10, 100)
+    assert np.array_equal(before, again)
     idx.close()
 
 
@@ -490,8 +498,9 @@ def test_graph_captured_uneven_plan(oracle_lib):
     from scattersearch_b200 import autotune
     choice = autotune.autotune(idx, q, total, 512, reps=1, path=None, Ks=dK, Ls=dL,
                                out_off=doff, wpb_candidates=(2, 8), hash_caps=(1024, 4096),
-                               shared_candidates=((8, 3),), stage_rows_candidates=(16,))
-    assert len(choice["table"]) == 6
+                               shared_candidates=((8, 3),), stage_rows_candidates=(16,),
+                               marks_off_top=2)
+    assert len(choice["table"]) == 8
     plan = idx.plan_batch_uneven_device(q, nq, dK, dL, doff, 512, ids, d)
     o_ids, o_d, _, _ = oracle_lib.search(fx["base"], fx["adj"], int(fx["ep"]), 0, Q, Ks=Ks, Ls=Ls)
     s = torch.cuda.current_stream()

@@ -175,31 +175,36 @@ def test_autotune_keys_and_cache(tmp_path):
 
 
 def test_autotune_apply_restores_the_whole_layout(tmp_path, monkeypatch):
-    """A cached choice sets teams per CTA, table size, stage rows and shared
-    stages on the index (a stand-in that records the call; no GPU)."""
+    """A cached choice sets teams per CTA, table size, stage rows, shared
+    stages and the visited-marks mode on the index (a stand-in that records
+    the calls; no GPU)."""
     from scattersearch_b200 import autotune as at
     monkeypatch.setattr(at, "_gpu_name", lambda device=None: "GPU-X")
 
     class FakeIndex:
         dimension, rstride = 96, 32
         calls = []
+        marks = []
 
         def set_tuning(self, *args):
             self.calls.append(args)
+
+        def set_visited_marks(self, mode):
+            self.marks.append(mode)
 
     path = str(tmp_path / "tuning.json")
     idx = FakeIndex()
     assert at.apply(idx, 300, path=path) is None and idx.calls == []
     at.save_choice(at.tuning_key("GPU-X", 96, 32, 300),
                    {"warps_per_block": 4, "hash_cap": 2048, "shared_stages": 3,
-                    "stage_rows": 12}, path)
+                    "stage_rows": 12, "visited_marks": 1}, path)
     assert at.apply(idx, 400, path=path)["hash_cap"] == 2048  # same L bucket (512)
-    assert idx.calls == [(4, 2048, 0, 3, 12)]
+    assert idx.calls == [(4, 2048, 0, 3, 12)] and idx.marks == [1]
     # choices cached before stage layouts existed still apply
     at.save_choice(at.tuning_key("GPU-X", 96, 32, 40), {"warps_per_block": 1, "hash_cap": 1024},
                    path)
     at.apply(idx, 40, path=path)
-    assert idx.calls[-1] == (1, 1024, 0, 0, 0)
+    assert idx.calls[-1] == (1, 1024, 0, 0, 0) and idx.marks[-1] == 0
     assert len(at.SHARED_CANDIDATES) and all(s < w for w, s in at.SHARED_CANDIDATES)
 
 
