@@ -104,8 +104,8 @@ def parse_args(argv=None):
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the id-parity record against the parity-built reference")
     ap.add_argument("--layout", default=None,
-                    help="fixed launch layout 'teams_per_cta,table_slots,shared_stages,stage_rows' "
-                         "instead of the autotuner's (profiling)")
+                    help="fixed launch layout 'teams_per_cta,table_slots,shared_stages,stage_rows"
+                         "[,marks_off]' instead of the autotuner's (profiling)")
     args = ap.parse_args(argv)
     if args.nq is None:
         args.nq = 100_000 if args.workload == "cfg4" else 10_000
@@ -679,6 +679,8 @@ def measure_config2(device, steps, warmup, nq=10000, sample=1000):
     K, L = w.K, max(w.L_list)
     idx = ANNSearch(dim, n, X, w.metric, base_on_device=True)
     idx.SetGraph(adj, ep)
+    from scattersearch_b200 import autotune
+    tune = autotune.autotune(idx, Q, K, L, reps=2, path=None)
     ids_d = torch.empty((nq, K), dtype=torch.int32, device=device)
     ndc_d = torch.empty(nq, dtype=torch.int32, device=device)
     hops_d = torch.empty(nq, dtype=torch.int32, device=device)
@@ -696,12 +698,21 @@ def measure_config2(device, steps, warmup, nq=10000, sample=1000):
     torch.cuda.synchronize()
     dev_ms = [a.elapsed_time(b) for a, b in evs]
     ids = ids_d.cpu().numpy().view(np.uint32)
-    # per-query evaluations and hops (an untimed pass)
+    # per-query evaluations and hops of the reference algorithm (an untimed
+    # pass with a visited set that forgets nothing), then the tuned layout
+    # again for the e2e calls
+    idx.set_visited_marks(idx.VISITED_MARKS_AUTO)
+    idx.set_tuning(hash_cap=65536)
     idx.search_batch_device(Q, nq, ids_d, None, K=K, L=L, ndc=ndc_d, hops=hops_d,
                             stream=st.cuda_stream)
     torch.cuda.synchronize()
     ndc = ndc_d.cpu().numpy().view(np.uint32).astype(np.float64)
     hops = hops_d.cpu().numpy().view(np.uint32).astype(np.float64)
+    if not np.array_equal(ids_d.cpu().numpy().view(np.uint32), ids):
+        raise RuntimeError("configuration 2: ids depend on the visited-table setting")
+    idx.set_tuning(tune["warps_per_block"], tune["hash_cap"], 0, tune["shared_stages"],
+                   tune["stage_rows"])
+    idx.set_visited_marks(tune["visited_marks"])
     e2e = []
     for i in range(warmup + steps):
         t1 = time.perf_counter()
@@ -720,6 +731,8 @@ def measure_config2(device, steps, warmup, nq=10000, sample=1000):
            "device_qps": nq / mean_s, "ms_per_batch": 1e3 * mean_s,
            "e2e_qps": nq * steps / sum(e2e),
            "ids_equal_e2e_device": bool(np.array_equal(h_ids, ids)),
+           "tuning": {k: tune[k] for k in ("warps_per_block", "shared_stages", "stage_rows",
+                                           "hash_cap", "visited_marks")},
            "recall@10_gpu": recall_at_10(ids, gt),
            "mean_degree": float((adj != 0xFFFFFFFF).sum(1).mean()),
            "roofline": {"bound": "hbm", "achieved": float(bytes_q.sum()) / mean_s / 1e9,
@@ -934,15 +947,16 @@ def run_ours(args):
     # launch layout (teams per CTA, visited-table size) tuned on a sample
     from scattersearch_b200 import autotune
     if args.layout:
-        wpb, hc, sh, rows = (int(x) for x in args.layout.split(","))
-        tune = {"warps_per_block": wpb, "hash_cap": hc, "shared_stages": sh, "stage_rows": rows,
-                "table": []}
+        v = [int(x) for x in args.layout.split(",")]
+        tune = {"warps_per_block": v[0], "hash_cap": v[1], "shared_stages": v[2],
+                "stage_rows": v[3], "visited_marks": v[4] if len(v) > 4 else 0, "table": []}
     else:
         tune = autotune.autotune(idx, wl["Q"], K, L, reps=2, path=None)
     for r in sorted(tune["table"], key=lambda r: r["ms"])[:6]:
         log(f"  layout {r}")
     log(f"tuned: {tune['warps_per_block']} teams per CTA, {tune['shared_stages']} shared stages "
-        f"(0 = one per team) of {tune['stage_rows']} rows, {tune['hash_cap']}-slot visited table")
+        f"(0 = one per team) of {tune['stage_rows']} rows, {tune['hash_cap']}-slot visited table, "
+        f"visited marks {'off' if tune.get('visited_marks') else 'on'}")
 
     Qd = wl["Q"]
     ids_d = torch.empty((nq, K), dtype=torch.int32, device=device)
@@ -962,6 +976,7 @@ def run_ours(args):
     # the reference algorithm's distance evaluations, taken with a visited
     # table large enough never to forget; the default table may forget ids
     # and evaluate them again, which the second pass counts.
+    idx.set_visited_marks(idx.VISITED_MARKS_AUTO)
     idx.set_tuning(hash_cap=65536)
     step(with_stats=True)
     torch.cuda.synchronize()
@@ -972,6 +987,7 @@ def run_ours(args):
     ids_exact = ids_d.cpu().numpy().copy()
     idx.set_tuning(tune["warps_per_block"], tune["hash_cap"], 0, tune["shared_stages"],
                    tune["stage_rows"])
+    idx.set_visited_marks(tune.get("visited_marks", 0))
     step(with_stats=True)
     torch.cuda.synchronize()
     ndc_dev = ndc_d.cpu().numpy().astype(np.int64)
@@ -1055,6 +1071,7 @@ def run_ours(args):
         if solo and not args.no_online and wl["metric"] == 1 else None
     idx.set_tuning(tune["warps_per_block"], tune["hash_cap"], 0, tune["shared_stages"],
                    tune["stage_rows"])
+    idx.set_visited_marks(tune.get("visited_marks", 0))
     config1 = measure_config1(device, args.steps, args.warmup) \
         if solo and not args.no_config1 and args.workload == "cfg3" and args.scale == 1.0 else None
     config2 = measure_config2(device, args.steps, args.warmup) \
@@ -1085,6 +1102,7 @@ def run_ours(args):
                               "shared_stages": tune["shared_stages"],
                               "stage_rows": tune["stage_rows"],
                               "hash_cap": tune["hash_cap"],
+                              "visited_marks": "off" if tune.get("visited_marks") else "on",
                               "sample": f"the {nq} bench queries (launch layout only)"}},
         "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": nq * dim * 4,
                 "d2h_bytes_per_step": nq * K * 8, "ids_equal_device_path": same_ids},
@@ -1182,7 +1200,8 @@ def uneven_record(args, wl, d, device, cpu_seconds):
     tune = autotune.autotune(idx, Qd, total, L_max, reps=2, path=None, Ks=dK, Ls=dL,
                              out_off=doff)
     log(f"tuned: {tune['warps_per_block']} teams per CTA, {tune['shared_stages']} shared stages "
-        f"(0 = one per team) of {tune['stage_rows']} rows, {tune['hash_cap']}-slot visited table")
+        f"(0 = one per team) of {tune['stage_rows']} rows, {tune['hash_cap']}-slot visited table, "
+        f"visited marks {'off' if tune.get('visited_marks') else 'on'}")
     ids_d = torch.empty(total, dtype=torch.int32, device=device)
     dist_d = torch.empty(total, dtype=torch.float32, device=device)
     ndc_d = torch.empty(nq, dtype=torch.int32, device=device)
@@ -1196,6 +1215,7 @@ def uneven_record(args, wl, d, device, cpu_seconds):
         if idx.batch_status():
             raise RuntimeError("device batch reported failed queries")
 
+    idx.set_visited_marks(idx.VISITED_MARKS_AUTO)
     idx.set_tuning(hash_cap=65536)  # exact distance-evaluation counts
     stats_pass()
     ndc = ndc_d.cpu().numpy().astype(np.int64)
@@ -1203,6 +1223,7 @@ def uneven_record(args, wl, d, device, cpu_seconds):
     ids_exact = ids_d.cpu().numpy().copy()
     idx.set_tuning(tune["warps_per_block"], tune["hash_cap"], 0, tune["shared_stages"],
                    tune["stage_rows"])
+    idx.set_visited_marks(tune.get("visited_marks", 0))
     stats_pass()
     ndc_dev = ndc_d.cpu().numpy().astype(np.int64)
     if not np.array_equal(ids_d.cpu().numpy(), ids_exact):
@@ -1291,7 +1312,8 @@ def uneven_record(args, wl, d, device, cpu_seconds):
                    "tuning": {"warps_per_block": tune["warps_per_block"],
                               "shared_stages": tune["shared_stages"],
                               "stage_rows": tune["stage_rows"],
-                              "hash_cap": tune["hash_cap"]}},
+                              "hash_cap": tune["hash_cap"],
+                              "visited_marks": "off" if tune.get("visited_marks") else "on"}},
         "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": nq * dim * 4,
                 "d2h_bytes_per_step": total * 8, "ids_equal_device_path": same_ids},
         "plain_gpu": {"value": plain_qps, "unit": "queries/s", "sample": ns,
